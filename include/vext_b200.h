@@ -1,0 +1,196 @@
+/*
+ * vext_b200 -- B200 (sm_100a) engine for the exact two-identical-site
+ * Lennard-Jones guest energy in a full triclinic periodic cell.
+ *
+ * C ABI only: plain pointers and sizes, no C++ or torch types.  Every entry
+ * returns 0 on success or a nonzero status; vext_last_error() gives a
+ * message for the calling thread's last failure.
+ *
+ * Units: Angstrom, Kelvin.  Cells are row-vector matrices (Cartesian =
+ * fractional @ cell, row k = lattice vector k), exactly the `cell` array of
+ * the reference's case dictionary (src/string_vext/cell.py:7-29).
+ */
+#ifndef VEXT_B200_H
+#define VEXT_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define VEXT_API __attribute__((visibility("default")))
+#else
+#define VEXT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  1-4 are the reference kernel's own codes
+ * (native/vext/kernel.cpp:11-41); 16 and above are new. */
+enum {
+    VEXT_OK = 0,
+    VEXT_ERR_SIZES = 1,          /* bad sizes / cutoff                          */
+    VEXT_ERR_STARTS = 2,         /* CSR starts decreasing (or negative)         */
+    VEXT_ERR_INDEX = 3,          /* CSR neighbour index outside [0, n_images)   */
+    VEXT_ERR_NONFINITE = 4,      /* non-finite energy                           */
+    VEXT_ERR_CUDA = 16,          /* CUDA runtime error (message has details)    */
+    VEXT_ERR_TIMEOUT = 17,       /* a bounded device wait gave up               */
+    VEXT_ERR_ARGUMENT = 18,      /* invalid argument to a new entry point       */
+    VEXT_ERR_CAPACITY = 19,      /* a documented size limit was exceeded        */
+    VEXT_ERR_MEMORY = 20         /* device or host allocation failed            */
+};
+
+/* ------------------------------------------------------------------------ */
+/* Drop-in replacement of the reference CPU kernel.
+ *
+ * Replaces `evaluate_reused_neighbors` of native/vext/kernel.cpp:5-10, bound
+ * by ctypes in src/string_vext/native.py:18-22 (argtypes 3 x c_int, c_double,
+ * 11 x c_void_p; restype c_int) and called per 512-center batch at
+ * native.py:60-64.  Same arguments, same meaning (all HOST buffers, the
+ * output written in place as [center][axis] FP64), same return codes 0-4.
+ * The sum runs on the current CUDA device in FP64 with the reference's
+ * operation order and no contraction, so outputs are bit-identical to the
+ * reference kernel's.  Codes 2 and 3 are checked on the host before any
+ * device work, in the reference's order; a negative starts[0] is reported as
+ * code 2.  Images and per-image coefficients are cached on the device
+ * between calls and re-uploaded whenever their contents change. */
+VEXT_API int evaluate_reused_neighbors(int n_centers, int n_axes, int n_images, double cutoff2,
+                              const double *centers, const double *axes, const double *images,
+                              const double *offsets, const double *coeff12, const double *coeff6,
+                              const double *shift, const double *floor2, const int64_t *starts,
+                              const int32_t *indices, double *output);
+
+/* Message describing the calling thread's last nonzero status. */
+VEXT_API const char *vext_last_error(void);
+
+/* ------------------------------------------------------------------------ */
+/* Systems: one framework + one symmetric two-site guest, resident on the
+ * current device.  Replaces the per-call set-up of ReusePotential /
+ * TriclinicSitePotential (src/string_vext/neighbor.py:10-30,
+ * physics.py:43-57): Lorentz-Berthelot mixing, coefficients
+ * c12 = 4 eps sigma^12, c6 = 4 eps sigma^6, shift = -4 eps ((sigma/rc)^12 -
+ * (sigma/rc)^6), floor2 = (0.1 sigma)^2, every lattice image within the
+ * cutoff (never minimum image). */
+typedef struct vext_system_s *vext_system;
+
+typedef struct {
+    double cell[9];          /* row-vector cell                              */
+    int n_atoms;             /* framework atoms (>= 1)                        */
+    const double *frac;      /* n_atoms x 3 fractional (wrapped mod 1 inside) */
+    const double *sigma;     /* n_atoms framework sigma (A)                   */
+    const double *epsilon;   /* n_atoms framework epsilon/kB (K)              */
+    double guest_sigma;      /* both guest sites (identical)                  */
+    double guest_epsilon;
+    double offsets[2];       /* signed site offsets along the director (A)    */
+    double cutoff;           /* LJ cutoff rc (A)                              */
+    double temperature;      /* K, for the marginal field                     */
+} vext_system_desc;
+
+VEXT_API int vext_system_create(const vext_system_desc *desc, vext_system *out);
+VEXT_API int vext_system_destroy(vext_system sys);
+
+/* Mark every cached region list of the system stale: the next call rebuilds
+ * it (into the same device allocation when it still fits). */
+VEXT_API int vext_system_invalidate(vext_system sys);
+
+/* Device times (CUDA events on the launching stream) of the system's most
+ * recent list build and of the most recent field call's main kernel and
+ * epilogue, in ms; waits for those events.  list_ms is 0 if no list was
+ * built since the previous query. */
+VEXT_API int vext_last_timings(vext_system sys, double *list_ms, double *kernel_ms,
+                               double *epilogue_ms);
+
+/* Precision modes. */
+enum {
+    VEXT_MODE_MIXED = 0,     /* FP64 for pairs nearer than r_split, FP32 beyond,
+                                FP64 re-evaluation of poses whose energy lies in
+                                the refinement band                           */
+    VEXT_MODE_FP64 = 1       /* every pair in FP64 (the GPU oracle kernel)     */
+};
+
+typedef struct {
+    int mode;                /* VEXT_MODE_*                                   */
+    double r_split;          /* A; <= 0 selects the default (8 A)             */
+    double band_lo, band_hi; /* refinement band for E (K); band_hi <= band_lo
+                                disables refinement; defaults via
+                                vext_default_options                          */
+    int centers_per_region;  /* 16 or 32; 0 = autotuned                       */
+    int reserved[4];
+} vext_options;
+
+VEXT_API void vext_default_options(vext_options *opt);
+
+/* Statistics of the last field call. */
+typedef struct {
+    int64_t poses;
+    int64_t regions;
+    int64_t list_entries;    /* sum of per-region list lengths                */
+    int64_t near_entries;
+    int64_t refined_poses;
+    double list_build_ms, kernel_ms, epilogue_ms;  /* device time (events)   */
+} vext_field_stats;
+
+/* Full Vext field on a size^3 fractional grid (centers ((i+.5)/S, ...),
+ * i slowest) x n_axes unit directors (HOST, n_axes x 3, as the reference
+ * normalises them, src/string_vext/native.py:33-35).  Replaces
+ * calculate_vext (src/string_vext/vext.py:21-43).  HOST outputs (any may be
+ * NULL):
+ *   orientation_K  float32 [n_axes][S][S][S]   (= E.T.reshape(O,S,S,S))
+ *   energy_f64     double  [S^3][n_axes]       (the reference's FP64 array)
+ *   marginal_K     float32 [S][S][S]  -T (logsumexp(-E/T) - log O)
+ *   site_K         float32 [2][S][S][S]  site-0 single-site field, twice
+ *   grid           float32 [S][S][S]  asinh(marginal_K / 1000)              */
+VEXT_API int vext_field(vext_system sys, int size, int n_axes, const double *axes,
+               const vext_options *opt, float *orientation_K, double *energy_f64,
+               float *marginal_K, float *site_K, float *grid, vext_field_stats *stats);
+
+/* Same, with DEVICE output pointers on the caller's stream (cudaStream_t
+ * passed as void*; NULL = legacy default stream).  The call returns once the
+ * work is enqueued and the region lists for (size, shape) exist. */
+VEXT_API int vext_field_device(vext_system sys, int size, int n_axes, const double *axes_host,
+                      const vext_options *opt, float *orientation_K, double *energy_f64,
+                      float *marginal_K, float *site_K, float *grid, void *stream);
+
+/* ------------------------------------------------------------------------ */
+/* Pose energies and the analytic adjoint for arbitrary poses.  A pose is a
+ * Cartesian center (A) and a quaternion q = (w, x, y, z), used normalised;
+ * the guest director is u = R(q) e_x and site s sits at center + o_s u.
+ * Replaces the String energy kernels Vext_cal_s0 / Vext_s0_deri_cal and the
+ * forward-difference gradient (native/string/source_code/global.h:1071-1128,
+ * 1141-1325).  Pair terms are recomputed in the adjoint, never stored.
+ * Outputs (any gradient pointer may be NULL):
+ *   energy         double [n]
+ *   grad_center    double [n][3]   dE/d(center), K/A
+ *   grad_quat      double [n][4]   dE/dq of E(q/|q|): the gradient projected
+ *                                  to the tangent space of the unit sphere
+ *   grad_director  double [n][3]   dE/du, K/A (u held free of the unit constraint)
+ * The *_device variant takes device pointers and a stream; the plain variant
+ * host pointers. */
+VEXT_API int vext_pose_energy_grad(vext_system sys, int n, const double *centers, const double *quats,
+                          const vext_options *opt, double *energy, double *grad_center,
+                          double *grad_quat, double *grad_director);
+VEXT_API int vext_pose_energy_grad_device(vext_system sys, int n, const double *centers,
+                                 const double *quats, const vext_options *opt, double *energy,
+                                 double *grad_center, double *grad_quat, double *grad_director,
+                                 void *stream);
+
+/* ------------------------------------------------------------------------ */
+/* Diagnostics. */
+
+/* Non-tensor FP32 FMA throughput of the current device (FLOP/s, FMA = 2),
+ * measured by a register-resident FFMA chain kernel; iterations controls
+ * the run length. */
+VEXT_API int vext_measure_fp32_peak(int iterations, double *flops_per_second);
+
+/* Exact FP64 number of (site, image) pairs closer than the cutoff over the
+ * size^3 x n_axes field (the algorithmic unit of work). */
+VEXT_API int vext_count_pairs(vext_system sys, int size, int n_axes, const double *axes,
+                              int64_t *pairs);
+
+/* Library version string. */
+VEXT_API const char *vext_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,142 @@
+"""ctypes binding of ``libvext_b200.so`` (the sm_100a library, C ABI in
+include/vext_b200.h).
+
+The library is built in-tree (``string_vext_b200/lib``); there is no CPU
+fallback: importing the bindings without the library, or calling a compute
+entry without a CUDA device, raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+PACKAGE = Path(__file__).resolve().parent
+LIB_PATH = Path(os.environ.get("VEXT_B200_LIBRARY", PACKAGE / "lib" / "libvext_b200.so"))
+
+VEXT_MODE_MIXED = 0
+VEXT_MODE_FP64 = 1
+
+STATUS = {0: "ok", 1: "bad sizes", 2: "CSR starts decreasing", 3: "CSR index out of range",
+          4: "non-finite energy", 16: "CUDA error", 17: "device wait timeout",
+          18: "invalid argument", 19: "capacity exceeded", 20: "out of memory"}
+
+
+class SystemDesc(ctypes.Structure):
+    _fields_ = [("cell", ctypes.c_double * 9), ("n_atoms", ctypes.c_int),
+                ("frac", ctypes.c_void_p), ("sigma", ctypes.c_void_p),
+                ("epsilon", ctypes.c_void_p), ("guest_sigma", ctypes.c_double),
+                ("guest_epsilon", ctypes.c_double), ("offsets", ctypes.c_double * 2),
+                ("cutoff", ctypes.c_double), ("temperature", ctypes.c_double)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int), ("r_split", ctypes.c_double),
+                ("band_lo", ctypes.c_double), ("band_hi", ctypes.c_double),
+                ("centers_per_region", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
+
+
+class FieldStats(ctypes.Structure):
+    _fields_ = [("poses", ctypes.c_int64), ("regions", ctypes.c_int64),
+                ("list_entries", ctypes.c_int64), ("near_entries", ctypes.c_int64),
+                ("refined_poses", ctypes.c_int64), ("list_build_ms", ctypes.c_double),
+                ("kernel_ms", ctypes.c_double), ("epilogue_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class VextError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"vext_b200 status {code} ({STATUS.get(code, '?')}): {message}")
+        self.code = code
+
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load the library once; raise if it is missing (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"vext_b200 CUDA library not built: {LIB_PATH} "
+                           "(run __graft_entry__.build() or make -C string_vext_b200/csrc)")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    vp, ci, cd = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    lib.evaluate_reused_neighbors.argtypes = [ci, ci, ci, cd] + [vp] * 11
+    lib.evaluate_reused_neighbors.restype = ci
+    lib.vext_last_error.argtypes = []
+    lib.vext_last_error.restype = ctypes.c_char_p
+    lib.vext_version.argtypes = []
+    lib.vext_version.restype = ctypes.c_char_p
+    lib.vext_default_options.argtypes = [ctypes.POINTER(Options)]
+    lib.vext_default_options.restype = None
+    lib.vext_system_create.argtypes = [ctypes.POINTER(SystemDesc), ctypes.POINTER(vp)]
+    lib.vext_system_create.restype = ci
+    lib.vext_system_destroy.argtypes = [vp]
+    lib.vext_system_destroy.restype = ci
+    lib.vext_field.argtypes = [vp, ci, ci, vp, ctypes.POINTER(Options), vp, vp, vp, vp, vp,
+                               ctypes.POINTER(FieldStats)]
+    lib.vext_field.restype = ci
+    lib.vext_field_device.argtypes = [vp, ci, ci, vp, ctypes.POINTER(Options), vp, vp, vp, vp,
+                                      vp, vp]
+    lib.vext_field_device.restype = ci
+    lib.vext_pose_energy_grad.argtypes = [vp, ci, vp, vp, ctypes.POINTER(Options), vp, vp, vp, vp]
+    lib.vext_pose_energy_grad.restype = ci
+    lib.vext_pose_energy_grad_device.argtypes = [vp, ci, vp, vp, ctypes.POINTER(Options), vp, vp,
+                                                 vp, vp, vp]
+    lib.vext_pose_energy_grad_device.restype = ci
+    lib.vext_system_invalidate.argtypes = [vp]
+    lib.vext_system_invalidate.restype = ci
+    lib.vext_last_timings.argtypes = [vp] + [ctypes.POINTER(ctypes.c_double)] * 3
+    lib.vext_last_timings.restype = ci
+    lib.vext_count_pairs.argtypes = [vp, ci, ci, vp, ctypes.POINTER(ctypes.c_int64)]
+    lib.vext_count_pairs.restype = ci
+    lib.vext_measure_fp32_peak.argtypes = [ci, ctypes.POINTER(ctypes.c_double)]
+    lib.vext_measure_fp32_peak.restype = ci
+    _lib = lib
+    return lib
+
+
+def check(code: int) -> None:
+    if code:
+        message = load().vext_last_error().decode(errors="replace")
+        raise VextError(code, message)
+
+
+def ptr(array) -> ctypes.c_void_p | None:
+    """Data pointer of a numpy array or torch tensor (None passes NULL)."""
+    if array is None:
+        return None
+    if isinstance(array, np.ndarray):
+        return ctypes.c_void_p(array.ctypes.data)
+    return ctypes.c_void_p(array.data_ptr())
+
+
+def options(mode: int = VEXT_MODE_MIXED, r_split: float | None = None,
+            band: tuple[float, float] | None = None,
+            centers_per_region: int | None = None) -> Options:
+    opt = Options()
+    load().vext_default_options(ctypes.byref(opt))
+    opt.mode = mode
+    if r_split is not None:
+        opt.r_split = r_split
+    if band is not None:
+        opt.band_lo, opt.band_hi = band
+    if centers_per_region is not None:
+        opt.centers_per_region = centers_per_region
+    return opt
+
+
+def version() -> str:
+    return load().vext_version().decode()
+
+
+def measure_fp32_peak(iterations: int = 20000) -> float:
+    value = ctypes.c_double()
+    check(load().vext_measure_fp32_peak(iterations, ctypes.byref(value)))
+    return value.value

@@ -1,0 +1,580 @@
+// Vext field kernels: every (grid center, director) pose of a size^3 grid.
+//
+// One CTA = one region (a block of CB grid centers) x one block of G*P
+// directors; thread (cl, og) owns center cl and directors og + G p
+// (p < P), i.e. 2P guest sites held in registers in FP64 and FP32,
+// relative to the region origin.  The region's list is streamed through
+// shared memory in kCH-entry chunks by bulk copies (stage.cuh); every staged
+// entry is used by all 2P sites of all threads.
+//
+// Precision: near chunks (entries within r_split + max|offset| + rho of the
+// origin) are evaluated in FP64 from the exact hi + lo positions; far chunks
+// in FP32 from hi, with an IEEE-rounded reciprocal refined by one Newton
+// step, accumulated in FP32 over 16 entries and then flushed into the FP64
+// per-site sum.  Poses whose energy falls in the refinement band (where the
+// 1e-6 relative criterion is tighter than the FP32 error) are recomputed in
+// FP64 by refine_kernel.  With r_split = infinity every entry is near: that
+// is the FP64 oracle kernel.
+//
+// Pair term (native/vext/kernel.cpp:26-36 and neighbor.py:21-28):
+//   d2 < rc^2:  s2 = max(d2, floor2), i6 = 1/s2^3, e = c12 i6^2 - c6 i6 + shift.
+#include <algorithm>
+#include <cmath>
+
+#include "stage.cuh"
+
+namespace vext {
+
+struct FieldArgs {
+    Mat3 H;
+    double rc2;
+    float rc2f;
+    double off0, off1;
+    int S, O;
+    const double *axes;       // device [O][3]
+    const RegionInfo *regs;
+    int n_regions;
+    int bi, bj, bk, nrj, nrk; // region grid (for pose -> region)
+    const float4 *hi, *lo;
+    const float4 *tf;
+    const double *td;
+    int n_types;
+    double *e64;              // [O][S^3]
+    int *status;
+};
+
+__device__ __forceinline__ void center_of(const FieldArgs &a, const RegionInfo &r, int cl,
+                                          int &gi, int &gj, int &gk) {
+    const int lk = cl % r.nk, lj = (cl / r.nk) % r.nj, li = cl / (r.nk * r.nj);
+    gi = r.i0 + li;
+    gj = r.j0 + lj;
+    gk = r.k0 + lk;
+}
+
+template <int CB, int G, int P>
+__global__ void __launch_bounds__(CB *G, 2) field_kernel(FieldArgs a) {
+    constexpr int NT = CB * G;
+    extern __shared__ __align__(128) unsigned char smem[];
+    Stager st;
+    st.bar = reinterpret_cast<uint64_t *>(smem);
+    st.hib = reinterpret_cast<float4 *>(smem + 64);
+    st.lob = st.hib + kStages * kCH;
+    double *ed = reinterpret_cast<double *>(st.lob + kStages * kCH);   // [kCH][4]
+    float4 *stf = reinterpret_cast<float4 *>(ed + 4 * kCH);
+    double *std4 = reinterpret_cast<double *>(stf + a.n_types);
+
+    const int tid = threadIdx.x;
+    const RegionInfo r = a.regs[blockIdx.x];
+    ChunkPlan plan;
+    plan.init(r);
+
+    for (int t = tid; t < a.n_types; t += NT) {
+        stf[t] = a.tf[t];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) std4[4 * t + k] = a.td[4 * t + k];
+    }
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) mbar_init(&st.bar[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int c = 0; c < min(kStages, plan.n_chunks); ++c) st.issue(plan, a.hi, a.lo, c, c);
+
+    // ---- this thread's poses (FP64 set-up relative to the region origin)
+    const int cl = tid % CB, og = tid / CB;
+    const int ncent = r.ni * r.nj * r.nk;
+    const bool cvalid = cl < ncent;
+    int gi, gj, gk;
+    center_of(a, r, cvalid ? cl : 0, gi, gj, gk);
+    double cx, cy, cz;
+    frac_to_cart(a.H, (gi + .5) / a.S - r.of[0], (gj + .5) / a.S - r.of[1],
+                 (gk + .5) / a.S - r.of[2], cx, cy, cz);
+    const int obase = blockIdx.y * (G * P) + og;
+    double sd[P][2][3];
+    float sf[P][2][3];
+    double acc[P][2];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        const int o = min(obase + G * p, a.O - 1);
+        const double ux = a.axes[3 * o], uy = a.axes[3 * o + 1], uz = a.axes[3 * o + 2];
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const double off = s ? a.off1 : a.off0;
+            sd[p][s][0] = cx + off * ux;
+            sd[p][s][1] = cy + off * uy;
+            sd[p][s][2] = cz + off * uz;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) sf[p][s][k] = (float)sd[p][s][k];
+            acc[p][s] = 0.0;
+        }
+    }
+
+    for (int c = 0; c < plan.n_chunks; ++c) {
+        const int s = c % kStages;
+        const bool ok = mbar_wait_bounded(&st.bar[s], (c / kStages) & 1, a.status);
+        if (!__syncthreads_and(ok)) {
+            if (tid == 0)   // let copies already in flight land before exiting
+                for (int cc = c; cc < min(c + kStages, plan.n_chunks); ++cc)
+                    mbar_drain(&st.bar[cc % kStages], (cc / kStages) & 1);
+            return;
+        }
+        int start, len;
+        bool near;
+        plan.chunk(c, start, len, near);
+        if (near) {
+            const float4 *hb = st.hib + s * kCH, *lb = st.lob + s * kCH;
+            for (int e = tid; e < len; e += NT) {
+                const float4 h = hb[e], l = lb[e];
+                ed[4 * e + 0] = (double)h.x + (double)l.x;
+                ed[4 * e + 1] = (double)h.y + (double)l.y;
+                ed[4 * e + 2] = (double)h.z + (double)l.z;
+                ed[4 * e + 3] = (double)__float_as_int(h.w);
+            }
+            __syncthreads();
+            const double2 *ed2 = reinterpret_cast<const double2 *>(ed);
+            const double2 *td2 = reinterpret_cast<const double2 *>(std4);
+#pragma unroll 1
+            for (int e = 0; e < len; ++e) {
+                const double2 xy = ed2[2 * e], zt = ed2[2 * e + 1];
+                const int t = (int)zt.y;
+                const double2 cc = td2[2 * t], sh = td2[2 * t + 1];   // (c12, c6), (shift, floor2)
+#pragma unroll
+                for (int p = 0; p < P; ++p)
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const double dx = sd[p][q][0] - xy.x, dy = sd[p][q][1] - xy.y,
+                                     dz = sd[p][q][2] - zt.x;
+                        const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
+                        const double s2 = fmax(d2, sh.y);
+                        const double i2 = __drcp_rn(s2);
+                        const double i6 = i2 * i2 * i2;
+                        const double en = fma(i6, fma(cc.x, i6, -cc.y), sh.x);
+                        acc[p][q] += d2 < a.rc2 ? en : 0.0;
+                    }
+            }
+        } else {
+            const float4 *hb = st.hib + s * kCH;
+#pragma unroll 1
+            for (int e0 = 0; e0 < len; e0 += 16) {
+                float fa[P][2];
+#pragma unroll
+                for (int p = 0; p < P; ++p) fa[p][0] = fa[p][1] = 0.f;
+                const int e1 = min(e0 + 16, len);
+#pragma unroll 2
+                for (int e = e0; e < e1; ++e) {
+                    const float4 h = hb[e];
+                    const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, floor2)
+#pragma unroll
+                    for (int p = 0; p < P; ++p)
+#pragma unroll
+                        for (int q = 0; q < 2; ++q) {
+                            const float dx = sf[p][q][0] - h.x, dy = sf[p][q][1] - h.y,
+                                        dz = sf[p][q][2] - h.z;
+                            const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                            const float s2 = fmaxf(d2, tp.w);
+                            const float i2 = rcp_nr(s2);
+                            const float i6 = i2 * i2 * i2;
+                            const float en = fmaf(i6, fmaf(tp.x, i6, -tp.y), tp.z);
+                            fa[p][q] += d2 < a.rc2f ? en : 0.f;
+                        }
+                }
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    acc[p][0] += (double)fa[p][0];
+                    acc[p][1] += (double)fa[p][1];
+                }
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && c + kStages < plan.n_chunks)
+            st.issue(plan, a.hi, a.lo, c + kStages, c + kStages);
+    }
+
+    if (cvalid) {
+        const size_t S3 = (size_t)a.S * a.S * a.S;
+        const size_t cg = ((size_t)gi * a.S + gj) * a.S + gk;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            const int o = obase + G * p;
+            if (o < a.O) a.e64[(size_t)o * S3 + cg] = acc[p][0] + acc[p][1];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- epilogue
+
+__global__ void flag_kernel(const double *e64, long long n, double lo, double hi, int *list) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double v = e64[i];
+        if (v > lo && v < hi) {
+            const int k = atomicAdd(&list[0], 1);
+            list[1 + k] = (int)i;
+        }
+    }
+}
+
+// FP64 pair sum of one site against one region's list, lane-strided over a
+// warp (no reduction here).
+__device__ __forceinline__ double site_sum_fp64(const FieldArgs &a, const RegionInfo &r,
+                                                double px, double py, double pz, int lane) {
+    double sum = 0.0;
+    for (int e = lane; e < r.n_total; e += 32) {
+        const float4 h = a.hi[r.off + e], l = a.lo[r.off + e];
+        const double dx = px - ((double)h.x + (double)l.x);
+        const double dy = py - ((double)h.y + (double)l.y);
+        const double dz = pz - ((double)h.z + (double)l.z);
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 < a.rc2) {
+            const int t = __float_as_int(h.w);
+            const double c12 = a.td[4 * t], c6 = a.td[4 * t + 1], shift = a.td[4 * t + 2],
+                         fl = a.td[4 * t + 3];
+            const double s2 = d2 < fl ? fl : d2;
+            const double i2 = 1.0 / s2;
+            const double i6 = i2 * i2 * i2;
+            sum += c12 * i6 * i6 - c6 * i6 + shift;
+        }
+    }
+    return sum;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ int region_of(const FieldArgs &a, int gi, int gj, int gk) {
+    return ((gi / a.bi) * a.nrj + gj / a.bj) * a.nrk + gk / a.bk;
+}
+
+__global__ void refine_kernel(FieldArgs a, const int *list) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int count = list[0];
+    const long long S3 = (long long)a.S * a.S * a.S;
+    for (int q = warp; q < count; q += nwarps) {
+        const long long idx = list[1 + q];
+        const int o = (int)(idx / S3);
+        const long long c = idx % S3;
+        const int gi = (int)(c / ((long long)a.S * a.S)), gj = (int)((c / a.S) % a.S),
+                  gk = (int)(c % a.S);
+        const RegionInfo r = a.regs[region_of(a, gi, gj, gk)];
+        double cx, cy, cz;
+        frac_to_cart(a.H, (gi + .5) / a.S - r.of[0], (gj + .5) / a.S - r.of[1],
+                     (gk + .5) / a.S - r.of[2], cx, cy, cz);
+        const double ux = a.axes[3 * o], uy = a.axes[3 * o + 1], uz = a.axes[3 * o + 2];
+        double e = site_sum_fp64(a, r, cx + a.off0 * ux, cy + a.off0 * uy, cz + a.off0 * uz, lane);
+        e += site_sum_fp64(a, r, cx + a.off1 * ux, cy + a.off1 * uy, cz + a.off1 * uz, lane);
+        e = warp_sum(e);
+        if (lane == 0) a.e64[idx] = e;
+    }
+}
+
+// Single-site field at the grid centers (site 0 parameters, no offset):
+// the reference's site_K (src/string_vext/vext.py:27-29, 33).
+__global__ void site_kernel(FieldArgs a, float *site_K) {
+    const int lane = threadIdx.x & 31;
+    const long long S3 = (long long)a.S * a.S * a.S;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < S3;
+         c += nwarps) {
+        const int gi = (int)(c / ((long long)a.S * a.S)), gj = (int)((c / a.S) % a.S),
+                  gk = (int)(c % a.S);
+        const RegionInfo r = a.regs[region_of(a, gi, gj, gk)];
+        double cx, cy, cz;
+        frac_to_cart(a.H, (gi + .5) / a.S - r.of[0], (gj + .5) / a.S - r.of[1],
+                     (gk + .5) / a.S - r.of[2], cx, cy, cz);
+        const double e = warp_sum(site_sum_fp64(a, r, cx, cy, cz, lane));
+        if (lane == 0) {
+            site_K[c] = (float)e;
+            site_K[S3 + c] = (float)e;
+        }
+    }
+}
+
+// Per center: float32 orientation field, marginal -T (logsumexp(-E/T) - log O)
+// (physics.py:126-130) and grid = asinh(marginal / 1000) (vext.py:40).
+__global__ void finalize_kernel(const double *e64, int S, int O, double T, float *orientation_K,
+                                float *marginal_K, float *grid, int *nonfinite) {
+    const long long S3 = (long long)S * S * S;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < S3;
+         c += (long long)gridDim.x * blockDim.x) {
+        double amax = -INFINITY;
+        bool finite = true;
+        for (int o = 0; o < O; ++o) {
+            const double e = e64[(long long)o * S3 + c];
+            finite = finite && isfinite(e);
+            if (orientation_K) orientation_K[(long long)o * S3 + c] = (float)e;
+            amax = fmax(amax, -e / T);
+        }
+        if (!finite) {
+            atomicAdd(nonfinite, 1);
+            continue;
+        }
+        if (marginal_K || grid) {
+            double sum = 0.0;
+            for (int o = 0; o < O; ++o) sum += exp(-e64[(long long)o * S3 + c] / T - amax);
+            const double m = -T * (log(sum) + amax - log((double)O));
+            const float m32 = (float)m;
+            if (marginal_K) marginal_K[c] = m32;
+            if (grid) grid[c] = (float)asinh((double)(m32 / 1000.0f));
+        }
+    }
+}
+
+// [O][S^3] -> [S^3][O] (the reference's (n_centers, n_axes) FP64 array).
+__global__ void transpose_kernel(const double *e64, long long S3, int O, double *out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < S3 * O;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long c = i / O;
+        const int o = (int)(i % O);
+        out[i] = e64[(long long)o * S3 + c];
+    }
+}
+
+// Exact FP64 count of in-cutoff (site, image) pairs over the whole field:
+// the algorithmic unit of work.  One warp per grid center, lanes over the
+// region's entries, every director and both sites tested per entry.
+__global__ void count_kernel(FieldArgs a, unsigned long long *total) {
+    const int lane = threadIdx.x & 31;
+    const long long S3 = (long long)a.S * a.S * a.S;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    unsigned long long mine = 0;
+    for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < S3;
+         c += nwarps) {
+        const int gi = (int)(c / ((long long)a.S * a.S)), gj = (int)((c / a.S) % a.S),
+                  gk = (int)(c % a.S);
+        const RegionInfo r = a.regs[region_of(a, gi, gj, gk)];
+        double cx, cy, cz;
+        frac_to_cart(a.H, (gi + .5) / a.S - r.of[0], (gj + .5) / a.S - r.of[1],
+                     (gk + .5) / a.S - r.of[2], cx, cy, cz);
+        for (int e = lane; e < r.n_total; e += 32) {
+            const float4 h = a.hi[r.off + e], l = a.lo[r.off + e];
+            const double x = (double)h.x + (double)l.x, y = (double)h.y + (double)l.y,
+                         z = (double)h.z + (double)l.z;
+            for (int o = 0; o < a.O; ++o) {
+                const double ux = a.axes[3 * o], uy = a.axes[3 * o + 1], uz = a.axes[3 * o + 2];
+                for (int s = 0; s < 2; ++s) {
+                    const double off = s ? a.off1 : a.off0;
+                    const double dx = cx + off * ux - x, dy = cy + off * uy - y,
+                                 dz = cz + off * uz - z;
+                    mine += (dx * dx + dy * dy + dz * dz) < a.rc2;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+    if (lane == 0) atomicAdd(total, mine);
+}
+
+// ---------------------------------------------------------------- launchers
+
+static size_t field_smem(int n_types) {
+    return kStageBytes + (size_t)kCH * 4 * sizeof(double) + (size_t)n_types * (16 + 32);
+}
+
+template <int CB, int G, int P>
+static int launch_field_t(const FieldArgs &a, cudaStream_t stream) {
+    const size_t smem = field_smem(a.n_types);
+    auto kern = field_kernel<CB, G, P>;
+    VEXT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid(a.n_regions, (a.O + G * P - 1) / (G * P));
+    kern<<<grid, CB * G, smem, stream>>>(a);
+    VEXT_CUDA(cudaGetLastError());
+    return 0;
+}
+
+static FieldArgs make_args(System *sys, const RegionSet *rs, int n_axes, const double *d_axes,
+                           double *d_e64) {
+    FieldArgs a;
+    a.H = sys->H;
+    a.rc2 = sys->cutoff * sys->cutoff;
+    a.rc2f = (float)a.rc2;
+    a.off0 = sys->offsets[0];
+    a.off1 = sys->offsets[1];
+    a.S = rs->size;
+    a.O = n_axes;
+    a.axes = d_axes;
+    a.regs = rs->d_info;
+    a.n_regions = rs->n_regions;
+    a.bi = rs->bi;
+    a.bj = rs->bj;
+    a.bk = rs->bk;
+    a.nrj = rs->n_rj;
+    a.nrk = rs->n_rk;
+    a.hi = rs->d_hi;
+    a.lo = rs->d_lo;
+    a.tf = sys->d_tf;
+    a.td = sys->d_td;
+    a.n_types = sys->n_types;
+    a.e64 = d_e64;
+    a.status = sys->d_status;
+    return a;
+}
+
+int launch_field(System *sys, const RegionSet *rs, int n_axes, const double *d_axes,
+                 double *d_e64, int cb, cudaStream_t stream) {
+    const FieldArgs a = make_args(sys, rs, n_axes, d_axes, d_e64);
+    if (cb == 32) return launch_field_t<32, 8, 4>(a, stream);
+    return launch_field_t<16, 16, 4>(a, stream);
+}
+
+// Everything on device pointers and `stream`; region lists are built (with
+// a host synchronisation) on first use of (size, shape, r_split).
+static int field_device(System *sys, int size, int n_axes, const double *axes_host,
+                        const Options &o, float *d_oK, double *d_e64_out, float *d_marg,
+                        float *d_site, float *d_grid, cudaStream_t stream,
+                        vext_field_stats *stats) {
+    if (size < 1 || n_axes < 1 || !axes_host)
+        return fail(VEXT_ERR_ARGUMENT, "size >= 1, n_axes >= 1 and axes required");
+    const long long S3 = (long long)size * size * size;
+    if (S3 * n_axes >= (1LL << 31) - 1)
+        return fail(VEXT_ERR_CAPACITY, "size^3 * n_axes must stay below 2^31");
+    for (int k = 0; k < 3 * n_axes; ++k)
+        if (!std::isfinite(axes_host[k])) return fail(VEXT_ERR_ARGUMENT, "non-finite director");
+    if (o.mode != VEXT_MODE_MIXED && o.mode != VEXT_MODE_FP64)
+        return fail(VEXT_ERR_ARGUMENT, "unknown precision mode %d", o.mode);
+    const int cb = o.cb == 32 ? 32 : 16;
+    const double r_split = o.mode == VEXT_MODE_FP64 ? 1e30 : o.r_split;
+    RegionSet *rs = nullptr;
+    VEXT_TRY(get_field_regions(sys, size, cb, r_split, &rs, stream));
+    const size_t n = (size_t)S3 * n_axes;
+    VEXT_TRY(ensure_capacity(sys->d_axes, sys->axes_cap, 3 * (size_t)n_axes));
+    VEXT_TRY(ensure_capacity(sys->d_e64, sys->e64_cap, n));
+    VEXT_TRY(ensure_capacity(sys->d_refine, sys->refine_cap, n + 1));
+    VEXT_TRY(ensure_capacity(sys->d_flags, sys->flags_cap, 4));
+    VEXT_CUDA(cudaMemcpyAsync(sys->d_axes, axes_host, sizeof(double) * 3 * n_axes,
+                              cudaMemcpyHostToDevice, stream));
+    VEXT_CUDA(cudaMemsetAsync(sys->d_flags, 0, sizeof(int) * 4, stream));
+    VEXT_CUDA(cudaMemsetAsync(sys->d_refine, 0, sizeof(int), stream));
+    const FieldArgs a = make_args(sys, rs, n_axes, sys->d_axes, sys->d_e64);
+    VEXT_CUDA(cudaEventRecord(sys->ev[0], stream));
+    VEXT_TRY(launch_field(sys, rs, n_axes, sys->d_axes, sys->d_e64, cb, stream));
+    VEXT_CUDA(cudaEventRecord(sys->ev[1], stream));
+    if (o.mode == VEXT_MODE_MIXED && o.band_hi > o.band_lo) {
+        flag_kernel<<<592, 256, 0, stream>>>(sys->d_e64, (long long)n, o.band_lo, o.band_hi,
+                                              sys->d_refine);
+        VEXT_CUDA(cudaGetLastError());
+        refine_kernel<<<1184, 256, 0, stream>>>(a, sys->d_refine);
+        VEXT_CUDA(cudaGetLastError());
+    }
+    if (d_site) {
+        site_kernel<<<1184, 256, 0, stream>>>(a, d_site);
+        VEXT_CUDA(cudaGetLastError());
+    }
+    finalize_kernel<<<592, 256, 0, stream>>>(sys->d_e64, size, n_axes, sys->temperature, d_oK,
+                                              d_marg, d_grid, sys->d_flags);
+    VEXT_CUDA(cudaGetLastError());
+    if (d_e64_out) {
+        transpose_kernel<<<1184, 256, 0, stream>>>(sys->d_e64, S3, n_axes, d_e64_out);
+        VEXT_CUDA(cudaGetLastError());
+    }
+    VEXT_CUDA(cudaEventRecord(sys->ev[2], stream));
+    sys->timed = true;
+    if (stats) {
+        VEXT_CUDA(cudaEventSynchronize(sys->ev[2]));
+        float k_ms = 0, e_ms = 0;
+        VEXT_CUDA(cudaEventElapsedTime(&k_ms, sys->ev[0], sys->ev[1]));
+        VEXT_CUDA(cudaEventElapsedTime(&e_ms, sys->ev[1], sys->ev[2]));
+        int refined = 0;
+        VEXT_CUDA(cudaMemcpy(&refined, sys->d_refine, sizeof(int), cudaMemcpyDeviceToHost));
+        stats->poses = (int64_t)n;
+        stats->regions = rs->n_regions;
+        stats->list_entries = rs->n_entries;
+        stats->near_entries = rs->n_near;
+        stats->refined_poses = o.mode == VEXT_MODE_MIXED && o.band_hi > o.band_lo ? refined : 0;
+        stats->list_build_ms = rs->build_ms;
+        stats->kernel_ms = k_ms;
+        stats->epilogue_ms = e_ms;
+    }
+    return 0;
+}
+
+static int check_nonfinite(System *sys, cudaStream_t stream) {
+    int h[2] = {0, 0};
+    VEXT_CUDA(cudaMemcpyAsync(h, sys->d_flags, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    VEXT_CUDA(cudaStreamSynchronize(stream));
+    if (h[0]) return fail(VEXT_ERR_NONFINITE, "%d grid centers with a non-finite energy", h[0]);
+    return check_status(sys, stream);
+}
+
+}  // namespace vext
+
+using namespace vext;
+
+extern "C" int vext_field(vext_system h, int size, int n_axes, const double *axes,
+                          const vext_options *opt, float *orientation_K, double *energy_f64,
+                          float *marginal_K, float *site_K, float *grid, vext_field_stats *stats) {
+    if (!h) return fail(VEXT_ERR_ARGUMENT, "null system");
+    System *sys = &h->sys;
+    std::lock_guard<std::mutex> guard(sys->lock);
+    VEXT_CUDA(cudaSetDevice(sys->device));
+    const Options o = resolve_options(opt);
+    const size_t S3 = (size_t)size * size * size, n = S3 * (size_t)(n_axes > 0 ? n_axes : 0);
+    cudaStream_t st = sys->stream;
+    if (orientation_K) VEXT_TRY(ensure_capacity(sys->d_f32, sys->f32_cap, n));
+    if (marginal_K || site_K || grid) VEXT_TRY(ensure_capacity(sys->d_small, sys->small_cap, 4 * S3));
+    if (energy_f64) VEXT_TRY(ensure_capacity(sys->d_e64T, sys->e64T_cap, n));
+    float *dm = marginal_K ? sys->d_small : nullptr;
+    float *ds = site_K ? sys->d_small + S3 : nullptr;
+    float *dg = grid ? sys->d_small + 3 * S3 : nullptr;
+    vext_field_stats local;
+    VEXT_TRY(field_device(sys, size, n_axes, axes, o, orientation_K ? sys->d_f32 : nullptr,
+                          energy_f64 ? sys->d_e64T : nullptr, dm, ds, dg, st,
+                          stats ? stats : &local));
+    if (orientation_K)
+        VEXT_CUDA(cudaMemcpyAsync(orientation_K, sys->d_f32, sizeof(float) * n,
+                                  cudaMemcpyDeviceToHost, st));
+    if (energy_f64)
+        VEXT_CUDA(cudaMemcpyAsync(energy_f64, sys->d_e64T, sizeof(double) * n,
+                                  cudaMemcpyDeviceToHost, st));
+    if (marginal_K)
+        VEXT_CUDA(cudaMemcpyAsync(marginal_K, dm, sizeof(float) * S3, cudaMemcpyDeviceToHost, st));
+    if (site_K)
+        VEXT_CUDA(cudaMemcpyAsync(site_K, ds, sizeof(float) * 2 * S3, cudaMemcpyDeviceToHost, st));
+    if (grid) VEXT_CUDA(cudaMemcpyAsync(grid, dg, sizeof(float) * S3, cudaMemcpyDeviceToHost, st));
+    return check_nonfinite(sys, st);
+}
+
+extern "C" int vext_field_device(vext_system h, int size, int n_axes, const double *axes_host,
+                                 const vext_options *opt, float *orientation_K,
+                                 double *energy_f64, float *marginal_K, float *site_K,
+                                 float *grid, void *stream) {
+    if (!h) return fail(VEXT_ERR_ARGUMENT, "null system");
+    System *sys = &h->sys;
+    std::lock_guard<std::mutex> guard(sys->lock);
+    VEXT_CUDA(cudaSetDevice(sys->device));
+    const Options o = resolve_options(opt);
+    return field_device(sys, size, n_axes, axes_host, o, orientation_K, energy_f64, marginal_K,
+                        site_K, grid, (cudaStream_t)stream, nullptr);
+}
+
+extern "C" int vext_count_pairs(vext_system h, int size, int n_axes, const double *axes,
+                                int64_t *pairs) {
+    if (!h || !pairs || !axes || size < 1 || n_axes < 1)
+        return fail(VEXT_ERR_ARGUMENT, "bad arguments");
+    System *sys = &h->sys;
+    std::lock_guard<std::mutex> guard(sys->lock);
+    VEXT_CUDA(cudaSetDevice(sys->device));
+    cudaStream_t st = sys->stream;
+    RegionSet *rs = nullptr;
+    VEXT_TRY(get_field_regions(sys, size, 16, 1e30, &rs, st));
+    VEXT_TRY(ensure_capacity(sys->d_axes, sys->axes_cap, 3 * (size_t)n_axes));
+    VEXT_TRY(ensure_capacity(sys->d_flags, sys->flags_cap, 4));
+    VEXT_CUDA(cudaMemcpyAsync(sys->d_axes, axes, sizeof(double) * 3 * n_axes,
+                              cudaMemcpyHostToDevice, st));
+    unsigned long long *total = reinterpret_cast<unsigned long long *>(sys->d_flags);
+    VEXT_CUDA(cudaMemsetAsync(total, 0, sizeof(unsigned long long), st));
+    const FieldArgs a = make_args(sys, rs, n_axes, sys->d_axes, nullptr);
+    count_kernel<<<2368, 256, 0, st>>>(a, total);
+    VEXT_CUDA(cudaGetLastError());
+    unsigned long long hcount = 0;
+    VEXT_CUDA(cudaMemcpyAsync(&hcount, total, sizeof hcount, cudaMemcpyDeviceToHost, st));
+    VEXT_CUDA(cudaStreamSynchronize(st));
+    *pairs = (int64_t)hcount;
+    return 0;
+}

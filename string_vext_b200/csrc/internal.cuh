@@ -1,0 +1,140 @@
+// Internal structures shared by the vext_b200 translation units.
+//
+// Data layout in HBM (per system = framework + guest):
+//   frac   double [n_atoms][3]   wrapped fractional coordinates
+//   type   int    [n_atoms]      index into the pair-parameter tables
+//   tf     float4 [n_types]      (c12, c6, shift, floor2) in FP32
+//   td     double [n_types][4]   the same in FP64 (reference arithmetic)
+// Per region set (one grid size + block shape, or the pose bins):
+//   info   RegionInfo [n_regions]
+//   hi     float4 [entries]  (x, y, z) of an image relative to the region
+//                            origin rounded to FP32; w = type id (int bits)
+//   lo     float4 [entries]  residual (x - hi.x, ...) so hi + lo is the FP64
+//                            relative position to ~1e-14 A
+// Each region's entries are contiguous (info.off), "near" entries first:
+// entries closer to the origin than r_split + max|offset| + rho are near,
+// so every (site, image) pair nearer than r_split has a near entry.
+#pragma once
+
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+
+namespace vext {
+
+constexpr int kMaxTypes = 1024;     // distinct framework (sigma, epsilon) pairs
+constexpr double kDefaultRSplit = 8.0;
+
+struct alignas(16) RegionInfo {
+    double of[3];       // origin, fractional
+    double rho;         // max distance (A) from the origin to any pose center
+    long long off;      // first entry
+    int n_near;         // near entries
+    int n_total;        // all entries
+    int i0, j0, k0;     // first grid center (field regions)
+    int ni, nj, nk;     // grid centers per axis (field regions)
+    int pad[2];
+};
+static_assert(sizeof(RegionInfo) % 16 == 0, "RegionInfo must stay 16-byte aligned");
+
+struct RegionSet {
+    // key
+    int size = 0, bi = 0, bj = 0, bk = 0;   // field regions (size > 0) or bins (size == 0)
+    int nb[3] = {0, 0, 0};                  // bins per axis (pose regions)
+    double r_split = 0;
+    // data
+    int n_regions = 0;
+    int n_ri = 0, n_rj = 0, n_rk = 0;       // regions per axis
+    long long n_entries = 0, n_near = 0;
+    RegionInfo *d_info = nullptr;
+    float4 *d_hi = nullptr, *d_lo = nullptr;
+    std::vector<RegionInfo> h_info;
+    long long capacity = 0;                 // allocated entries (hi and lo)
+    bool stale = false;                     // rebuild before the next use
+    float build_ms = 0;
+    ~RegionSet();
+};
+
+struct System {
+    int device = 0;
+    Mat3 H, Hinv;
+    double einv[3];        // |column k of Hinv| = 1 / lattice-plane spacing
+    int n_atoms = 0, n_types = 0;
+    double guest_sigma = 0, guest_epsilon = 0, offsets[2] = {0, 0}, cutoff = 0, temperature = 0;
+    double max_offset = 0;
+    double *d_frac = nullptr;
+    int *d_type = nullptr;
+    float4 *d_tf = nullptr;
+    double *d_td = nullptr;
+    std::vector<double> h_td;  // n_types x 4
+    std::vector<RegionSet *> sets;
+    int *d_status = nullptr;   // device status word
+    // scratch of the field path
+    double *d_e64 = nullptr;
+    size_t e64_cap = 0;
+    int *d_refine = nullptr;   // [0] = count, then pose indices
+    size_t refine_cap = 0;
+    double *d_axes = nullptr;
+    size_t axes_cap = 0;
+    float *d_f32 = nullptr;        // host-output staging of the float32 field
+    size_t f32_cap = 0;
+    float *d_small = nullptr;      // marginal, 2 x site, grid
+    size_t small_cap = 0;
+    double *d_e64T = nullptr;      // [S^3][O] FP64 output staging
+    size_t e64T_cap = 0;
+    int *d_flags = nullptr;        // [0] non-finite count
+    size_t flags_cap = 0;
+    // scratch of the pose path
+    void *d_pose_scratch = nullptr;
+    size_t pose_scratch_cap = 0;
+    cudaStream_t stream = nullptr;   // private stream for host-pointer entries
+    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    bool timed = false;              // ev[0..2] hold the last field call's kernel/epilogue
+    bool list_timed = false;         // ev[3..4] hold the last list build
+    std::mutex lock;
+    ~System();
+};
+
+// Region sets (system.cu)
+int get_field_regions(System *sys, int size, int cb, double r_split, RegionSet **out,
+                      cudaStream_t stream);
+int get_bin_regions(System *sys, double r_split, RegionSet **out, cudaStream_t stream);
+void choose_block_shape(const Mat3 &H, int size, int cb, int &bi, int &bj, int &bk);
+double block_radius(const Mat3 &H, int size, int ni, int nj, int nk);
+
+// Device buffer growth helper
+template <typename T>
+int ensure_capacity(T *&ptr, size_t &cap, size_t need) {
+    if (need <= cap && ptr) return 0;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    size_t n = need < 1 ? 1 : need;
+    cudaError_t err = cudaMalloc((void **)&ptr, n * sizeof(T));
+    if (err != cudaSuccess)
+        return fail(VEXT_ERR_MEMORY, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T),
+                    cudaGetErrorString(err));
+    cap = n;
+    return 0;
+}
+
+int check_status(System *sys, cudaStream_t stream);  // reads and clears the status word
+
+struct Options {
+    int mode;
+    double r_split;
+    double band_lo, band_hi;
+    int cb;
+};
+Options resolve_options(const vext_options *opt);
+
+// Field kernel launcher (field.cu): computes E64 [O][S^3] for all regions.
+int launch_field(System *sys, const RegionSet *rs, int n_axes, const double *d_axes,
+                 double *d_e64, int cb, cudaStream_t stream);
+
+}  // namespace vext
+
+struct vext_system_s {
+    vext::System sys;
+};

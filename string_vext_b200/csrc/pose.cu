@@ -1,0 +1,547 @@
+// Pose energies and the analytic adjoint for arbitrary poses (String images,
+// random pose batches, the torch autograd path).
+//
+// Poses are wrapped into the cell (FP64) and binned on a fractional grid of
+// ~2 A bins; every bin is a region with its own list (built once per system,
+// system.cu).  One CTA = one work item (a bin and up to kPoseThreads of its
+// poses, one pose per thread).  Pair terms are recomputed, never stored:
+//   E   = sum  c12 i6^2 - c6 i6 + shift                 (d2 < rc^2)
+//   dE/dr_site = sum i2 i6 (6 c6 - 12 c12 i6) (r_site - x)  (floor2 < d2 < rc^2)
+// (inside the contact floor the energy is constant, so its gradient is 0).
+// dE/dcenter = F0 + F1, dE/du = o0 F0 + o1 F1, and dE/dq = J(q)^T dE/du
+// projected onto the tangent space of the unit quaternion sphere, with
+// u = R(q) e_x = (1 - 2(y^2 + z^2), 2(xy + wz), 2(xz - wy)).
+// Precision follows the field kernel: near chunks FP64, far chunks FP32 with
+// periodic FP64 flushes, FP64 re-evaluation of poses in the refinement band.
+#include <algorithm>
+#include <cmath>
+
+#include "stage.cuh"
+
+namespace vext {
+
+constexpr int kPoseThreads = 128;
+
+struct PoseArgs {
+    Mat3 H, Hinv;
+    double rc2;
+    float rc2f;
+    double off0, off1;
+    int n;
+    const double *centers;   // [n][3] Cartesian
+    const double *quats;     // [n][4]
+    double *wf;              // [n][3] wrapped fractional
+    double *u;               // [n][3] director
+    int *bin;                // [n]
+    int nb0, nb1, nb2, n_bins;
+    int *counts, *starts, *cursor;   // [n_bins], [n_bins + 1], [n_bins]
+    int *order;              // [n] pose ids sorted by bin
+    int *items;              // [0] = count, then (bin, first, len)
+    int max_items;
+    const RegionInfo *regs;
+    const float4 *hi, *lo;
+    const float4 *tf;
+    const double *td;
+    int n_types;
+    double *energy, *gc, *gq, *gu;
+    int *refine;             // [0] = count, then pose ids
+    double band_lo, band_hi;
+    int *status;
+};
+
+enum : int { DEV_BAD_INPUT = 3 };
+
+__global__ void pose_prep_kernel(PoseArgs a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.n) return;
+    const double *q = a.quats + 4 * p;
+    const double nq = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    const double w = q[0] / nq, x = q[1] / nq, y = q[2] / nq, z = q[3] / nq;
+    a.u[3 * p + 0] = 1.0 - 2.0 * (y * y + z * z);
+    a.u[3 * p + 1] = 2.0 * (x * y + w * z);
+    a.u[3 * p + 2] = 2.0 * (x * z - w * y);
+    const double c0 = a.centers[3 * p], c1 = a.centers[3 * p + 1], c2 = a.centers[3 * p + 2];
+    double f[3];
+    int b[3];
+    const int nb[3] = {a.nb0, a.nb1, a.nb2};
+    bool ok = isfinite(nq) && nq > 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double v = c0 * a.Hinv.m[k] + c1 * a.Hinv.m[3 + k] + c2 * a.Hinv.m[6 + k];
+        ok = ok && isfinite(v);
+        v = isfinite(v) ? v - floor(v) : 0.0;
+        if (v >= 1.0) v = 0.0;
+        f[k] = v;
+        b[k] = min(nb[k] - 1, (int)(v * nb[k]));
+        a.wf[3 * p + k] = v;
+    }
+    if (!ok) atomicExch(a.status, DEV_BAD_INPUT);
+    const int id = (b[0] * a.nb1 + b[1]) * a.nb2 + b[2];
+    a.bin[p] = id;
+    atomicAdd(&a.counts[id], 1);
+}
+
+// Single CTA: bin starts and the (bin, first, len) work items.
+__global__ void pose_scan_kernel(PoseArgs a) {
+    __shared__ int carry[2];
+    __shared__ int warp_tot[2][32];
+    if (threadIdx.x == 0) carry[0] = carry[1] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int base = 0; base < a.n_bins; base += blockDim.x) {
+        const int b = base + threadIdx.x;
+        const int cnt = b < a.n_bins ? a.counts[b] : 0;
+        const int nit = (cnt + kPoseThreads - 1) / kPoseThreads;
+        int xc = cnt, xi = nit;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int yc = __shfl_up_sync(0xffffffffu, xc, o), yi = __shfl_up_sync(0xffffffffu, xi, o);
+            if (lane >= o) {
+                xc += yc;
+                xi += yi;
+            }
+        }
+        if (lane == 31) {
+            warp_tot[0][warp] = xc;
+            warp_tot[1][warp] = xi;
+        }
+        __syncthreads();
+        int wc = 0, wi = 0;
+        for (int w = 0; w < warp; ++w) {
+            wc += warp_tot[0][w];
+            wi += warp_tot[1][w];
+        }
+        const int pc = carry[0] + wc + xc - cnt, pi = carry[1] + wi + xi - nit;
+        if (b < a.n_bins) {
+            a.starts[b] = pc;
+            for (int k = 0; k < nit; ++k) {
+                const int it = pi + k;
+                if (it < a.max_items) {
+                    a.items[1 + 3 * it] = b;
+                    a.items[2 + 3 * it] = pc + k * kPoseThreads;
+                    a.items[3 + 3 * it] = min(kPoseThreads, cnt - k * kPoseThreads);
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int tc = 0, ti = 0;
+            for (int w = 0; w < nw; ++w) {
+                tc += warp_tot[0][w];
+                ti += warp_tot[1][w];
+            }
+            carry[0] += tc;
+            carry[1] += ti;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        a.starts[a.n_bins] = carry[0];
+        a.items[0] = min(carry[1], a.max_items);
+    }
+}
+
+__global__ void pose_scatter_kernel(PoseArgs a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.n) return;
+    const int b = a.bin[p];
+    a.order[a.starts[b] + atomicAdd(&a.cursor[b], 1)] = p;
+}
+
+__device__ __forceinline__ void write_pose(const PoseArgs &a, int p, double e, const double *F0,
+                                           const double *F1) {
+    if (a.energy) a.energy[p] = e;
+    if (a.gc)
+        for (int k = 0; k < 3; ++k) a.gc[3 * p + k] = F0[k] + F1[k];
+    double gu[3];
+    for (int k = 0; k < 3; ++k) gu[k] = a.off0 * F0[k] + a.off1 * F1[k];
+    if (a.gu)
+        for (int k = 0; k < 3; ++k) a.gu[3 * p + k] = gu[k];
+    if (a.gq) {
+        const double *q = a.quats + 4 * p;
+        const double nq = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+        const double w = q[0] / nq, x = q[1] / nq, y = q[2] / nq, z = q[3] / nq;
+        double g[4];
+        g[0] = 2 * z * gu[1] - 2 * y * gu[2];
+        g[1] = 2 * y * gu[1] + 2 * z * gu[2];
+        g[2] = -4 * y * gu[0] + 2 * x * gu[1] - 2 * w * gu[2];
+        g[3] = -4 * z * gu[0] + 2 * w * gu[1] + 2 * x * gu[2];
+        const double dot = g[0] * w + g[1] * x + g[2] * y + g[3] * z;
+        a.gq[4 * p + 0] = (g[0] - dot * w) / nq;
+        a.gq[4 * p + 1] = (g[1] - dot * x) / nq;
+        a.gq[4 * p + 2] = (g[2] - dot * y) / nq;
+        a.gq[4 * p + 3] = (g[3] - dot * z) / nq;
+    }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) pose_kernel(PoseArgs a) {
+    const int item = blockIdx.x;
+    if (item >= a.items[0]) return;   // uniform over the CTA
+    extern __shared__ __align__(128) unsigned char smem[];
+    Stager st;
+    st.bar = reinterpret_cast<uint64_t *>(smem);
+    st.hib = reinterpret_cast<float4 *>(smem + 64);
+    st.lob = st.hib + kStages * kCH;
+    double *ed = reinterpret_cast<double *>(st.lob + kStages * kCH);
+    float4 *stf = reinterpret_cast<float4 *>(ed + 4 * kCH);
+    double *std4 = reinterpret_cast<double *>(stf + a.n_types);
+
+    const int tid = threadIdx.x;
+    const int bin = a.items[1 + 3 * item], first = a.items[2 + 3 * item],
+              len_p = a.items[3 + 3 * item];
+    const RegionInfo r = a.regs[bin];
+    ChunkPlan plan;
+    plan.init(r);
+    for (int t = tid; t < a.n_types; t += NT) {
+        stf[t] = a.tf[t];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) std4[4 * t + k] = a.td[4 * t + k];
+    }
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) mbar_init(&st.bar[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int c = 0; c < min(kStages, plan.n_chunks); ++c) st.issue(plan, a.hi, a.lo, c, c);
+
+    const bool valid = tid < len_p;
+    const int p = a.order[first + (valid ? tid : 0)];
+    double cx, cy, cz;
+    frac_to_cart(a.H, a.wf[3 * p] - r.of[0], a.wf[3 * p + 1] - r.of[1], a.wf[3 * p + 2] - r.of[2],
+                 cx, cy, cz);
+    const double ux = a.u[3 * p], uy = a.u[3 * p + 1], uz = a.u[3 * p + 2];
+    double sd[2][3];
+    float sf[2][3];
+    double E[2] = {0, 0}, F[2][3] = {{0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        const double off = s ? a.off1 : a.off0;
+        sd[s][0] = cx + off * ux;
+        sd[s][1] = cy + off * uy;
+        sd[s][2] = cz + off * uz;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) sf[s][k] = (float)sd[s][k];
+    }
+
+    for (int c = 0; c < plan.n_chunks; ++c) {
+        const int s = c % kStages;
+        const bool ok = mbar_wait_bounded(&st.bar[s], (c / kStages) & 1, a.status);
+        if (!__syncthreads_and(ok)) {
+            if (tid == 0)
+                for (int cc = c; cc < min(c + kStages, plan.n_chunks); ++cc)
+                    mbar_drain(&st.bar[cc % kStages], (cc / kStages) & 1);
+            return;
+        }
+        int start, len;
+        bool near;
+        plan.chunk(c, start, len, near);
+        if (near) {
+            const float4 *hb = st.hib + s * kCH, *lb = st.lob + s * kCH;
+            for (int e = tid; e < len; e += NT) {
+                const float4 h = hb[e], l = lb[e];
+                ed[4 * e + 0] = (double)h.x + (double)l.x;
+                ed[4 * e + 1] = (double)h.y + (double)l.y;
+                ed[4 * e + 2] = (double)h.z + (double)l.z;
+                ed[4 * e + 3] = (double)__float_as_int(h.w);
+            }
+            __syncthreads();
+            const double2 *ed2 = reinterpret_cast<const double2 *>(ed);
+            const double2 *td2 = reinterpret_cast<const double2 *>(std4);
+#pragma unroll 1
+            for (int e = 0; e < len; ++e) {
+                const double2 xy = ed2[2 * e], zt = ed2[2 * e + 1];
+                const int t = (int)zt.y;
+                const double2 cc = td2[2 * t], sh = td2[2 * t + 1];
+                const double a12 = -12.0 * cc.x, a6 = 6.0 * cc.y;
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const double dx = sd[q][0] - xy.x, dy = sd[q][1] - xy.y, dz = sd[q][2] - zt.x;
+                    const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
+                    const double s2 = fmax(d2, sh.y);
+                    const double i2 = __drcp_rn(s2);
+                    const double i6 = i2 * i2 * i2;
+                    const double en = fma(i6, fma(cc.x, i6, -cc.y), sh.x);
+                    const bool in = d2 < a.rc2;
+                    const double w = (in && d2 > sh.y) ? i2 * i6 * fma(a12, i6, a6) : 0.0;
+                    E[q] += in ? en : 0.0;
+                    F[q][0] = fma(w, dx, F[q][0]);
+                    F[q][1] = fma(w, dy, F[q][1]);
+                    F[q][2] = fma(w, dz, F[q][2]);
+                }
+            }
+        } else {
+            const float4 *hb = st.hib + s * kCH;
+#pragma unroll 1
+            for (int e0 = 0; e0 < len; e0 += 16) {
+                float fe[2] = {0.f, 0.f}, ff[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+                const int e1 = min(e0 + 16, len);
+#pragma unroll 2
+                for (int e = e0; e < e1; ++e) {
+                    const float4 h = hb[e];
+                    const float4 tp = stf[__float_as_int(h.w)];
+                    const float a12 = -12.0f * tp.x, a6 = 6.0f * tp.y;
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const float dx = sf[q][0] - h.x, dy = sf[q][1] - h.y, dz = sf[q][2] - h.z;
+                        const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        const float s2 = fmaxf(d2, tp.w);
+                        const float i2 = rcp_nr(s2);
+                        const float i6 = i2 * i2 * i2;
+                        const float en = fmaf(i6, fmaf(tp.x, i6, -tp.y), tp.z);
+                        const bool in = d2 < a.rc2f;
+                        const float w = (in && d2 > tp.w) ? i2 * i6 * fmaf(a12, i6, a6) : 0.f;
+                        fe[q] += in ? en : 0.f;
+                        ff[q][0] = fmaf(w, dx, ff[q][0]);
+                        ff[q][1] = fmaf(w, dy, ff[q][1]);
+                        ff[q][2] = fmaf(w, dz, ff[q][2]);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    E[q] += (double)fe[q];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) F[q][k] += (double)ff[q][k];
+                }
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && c + kStages < plan.n_chunks)
+            st.issue(plan, a.hi, a.lo, c + kStages, c + kStages);
+    }
+    if (valid) {
+        const double e = E[0] + E[1];
+        write_pose(a, p, e, F[0], F[1]);
+        if (a.refine && e > a.band_lo && e < a.band_hi) {
+            const int k = atomicAdd(&a.refine[0], 1);
+            a.refine[1 + k] = p;
+        }
+    }
+}
+
+// FP64 re-evaluation of flagged poses, one warp per pose.
+__global__ void pose_refine_kernel(PoseArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int count = a.refine[0];
+    for (int q = warp; q < count; q += nwarps) {
+        const int p = a.refine[1 + q];
+        const RegionInfo r = a.regs[a.bin[p]];
+        double cx, cy, cz;
+        frac_to_cart(a.H, a.wf[3 * p] - r.of[0], a.wf[3 * p + 1] - r.of[1],
+                     a.wf[3 * p + 2] - r.of[2], cx, cy, cz);
+        const double ux = a.u[3 * p], uy = a.u[3 * p + 1], uz = a.u[3 * p + 2];
+        double v[7] = {0, 0, 0, 0, 0, 0, 0};   // E, F0 (3), F1 (3)
+        for (int s = 0; s < 2; ++s) {
+            const double off = s ? a.off1 : a.off0;
+            const double px = cx + off * ux, py = cy + off * uy, pz = cz + off * uz;
+            for (int e = lane; e < r.n_total; e += 32) {
+                const float4 h = a.hi[r.off + e], l = a.lo[r.off + e];
+                const double dx = px - ((double)h.x + (double)l.x);
+                const double dy = py - ((double)h.y + (double)l.y);
+                const double dz = pz - ((double)h.z + (double)l.z);
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                if (d2 >= a.rc2) continue;
+                const int t = __float_as_int(h.w);
+                const double c12 = a.td[4 * t], c6 = a.td[4 * t + 1], shift = a.td[4 * t + 2],
+                             fl = a.td[4 * t + 3];
+                const double s2 = d2 < fl ? fl : d2;
+                const double i2 = 1.0 / s2;
+                const double i6 = i2 * i2 * i2;
+                v[0] += c12 * i6 * i6 - c6 * i6 + shift;
+                if (d2 > fl) {
+                    const double w = i2 * i6 * (6.0 * c6 - 12.0 * c12 * i6);
+                    v[1 + 3 * s] += w * dx;
+                    v[2 + 3 * s] += w * dy;
+                    v[3 + 3 * s] += w * dz;
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 7; ++k)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+        if (lane == 0) write_pose(a, p, v[0], v + 1, v + 4);
+    }
+}
+
+// ---------------------------------------------------------------- host side
+
+struct Bump {
+    char *base;
+    size_t used = 0;
+    template <typename T>
+    T *take(size_t n) {
+        used = (used + 255) & ~(size_t)255;
+        T *p = reinterpret_cast<T *>(base + used);
+        used += n * sizeof(T);
+        return p;
+    }
+};
+
+static size_t pose_scratch_bytes(int n, int n_bins, int max_items, bool host_io) {
+    size_t b = 0;
+    auto add = [&](size_t bytes) { b = ((b + 255) & ~(size_t)255) + bytes; };
+    add(sizeof(double) * 3 * n);          // wf
+    add(sizeof(double) * 3 * n);          // u
+    add(sizeof(int) * n);                 // bin
+    add(sizeof(int) * n);                 // order
+    add(sizeof(int) * n_bins);            // counts
+    add(sizeof(int) * (n_bins + 1));      // starts
+    add(sizeof(int) * n_bins);            // cursor
+    add(sizeof(int) * (1 + 3 * (size_t)max_items));
+    add(sizeof(int) * (n + 1));           // refine
+    add(sizeof(double) * n);              // energy (when the caller passes none)
+    if (host_io) {
+        add(sizeof(double) * 3 * n);      // centers
+        add(sizeof(double) * 4 * n);      // quats
+        add(sizeof(double) * 3 * n);      // gc
+        add(sizeof(double) * 4 * n);      // gq
+        add(sizeof(double) * 3 * n);      // gu
+    }
+    return b + 256;
+}
+
+static int pose_run(System *sys, int n, const double *centers, const double *quats,
+                    const Options &o, double *energy, double *gc, double *gq, double *gu,
+                    cudaStream_t st, bool host_io) {
+    if (n < 0) return fail(VEXT_ERR_ARGUMENT, "negative pose count");
+    if (n == 0) return 0;
+    if (!centers || !quats) return fail(VEXT_ERR_ARGUMENT, "centers and quaternions required");
+    if (o.mode != VEXT_MODE_MIXED && o.mode != VEXT_MODE_FP64)
+        return fail(VEXT_ERR_ARGUMENT, "unknown precision mode %d", o.mode);
+    const double r_split = o.mode == VEXT_MODE_FP64 ? 1e30 : o.r_split;
+    RegionSet *rs = nullptr;
+    VEXT_TRY(get_bin_regions(sys, r_split, &rs, st));
+    const int n_bins = rs->n_regions;
+    const int max_items = n_bins + (n + kPoseThreads - 1) / kPoseThreads;
+    const size_t bytes = pose_scratch_bytes(n, n_bins, max_items, host_io);
+    VEXT_TRY(ensure_capacity(*reinterpret_cast<char **>(&sys->d_pose_scratch),
+                             sys->pose_scratch_cap, bytes));
+    Bump bump{reinterpret_cast<char *>(sys->d_pose_scratch)};
+    PoseArgs a;
+    a.H = sys->H;
+    a.Hinv = sys->Hinv;
+    a.rc2 = sys->cutoff * sys->cutoff;
+    a.rc2f = (float)a.rc2;
+    a.off0 = sys->offsets[0];
+    a.off1 = sys->offsets[1];
+    a.n = n;
+    a.wf = bump.take<double>(3 * (size_t)n);
+    a.u = bump.take<double>(3 * (size_t)n);
+    a.bin = bump.take<int>(n);
+    a.order = bump.take<int>(n);
+    a.nb0 = rs->nb[0];
+    a.nb1 = rs->nb[1];
+    a.nb2 = rs->nb[2];
+    a.n_bins = n_bins;
+    a.counts = bump.take<int>(n_bins);
+    a.starts = bump.take<int>(n_bins + 1);
+    a.cursor = bump.take<int>(n_bins);
+    a.items = bump.take<int>(1 + 3 * (size_t)max_items);
+    a.max_items = max_items;
+    a.regs = rs->d_info;
+    a.hi = rs->d_hi;
+    a.lo = rs->d_lo;
+    a.tf = sys->d_tf;
+    a.td = sys->d_td;
+    a.n_types = sys->n_types;
+    const bool refine = o.mode == VEXT_MODE_MIXED && o.band_hi > o.band_lo;
+    int *d_refine = bump.take<int>((size_t)n + 1);
+    a.refine = refine ? d_refine : nullptr;
+    a.band_lo = o.band_lo;
+    a.band_hi = o.band_hi;
+    a.status = sys->d_status;
+    double *e_tmp = bump.take<double>(n);
+    const double *in_c = centers, *in_q = quats;
+    double *out_gc = gc, *out_gq = gq, *out_gu = gu;
+    if (host_io) {
+        double *dc = bump.take<double>(3 * (size_t)n), *dq = bump.take<double>(4 * (size_t)n);
+        VEXT_CUDA(cudaMemcpyAsync(dc, centers, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+        VEXT_CUDA(cudaMemcpyAsync(dq, quats, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, st));
+        in_c = dc;
+        in_q = dq;
+        double *dgc = bump.take<double>(3 * (size_t)n), *dgq = bump.take<double>(4 * (size_t)n),
+               *dgu = bump.take<double>(3 * (size_t)n);
+        out_gc = gc ? dgc : nullptr;
+        out_gq = gq ? dgq : nullptr;
+        out_gu = gu ? dgu : nullptr;
+    }
+    a.centers = in_c;
+    a.quats = in_q;
+    a.energy = (energy && !host_io) ? energy : e_tmp;
+    a.gc = out_gc;
+    a.gq = out_gq;
+    a.gu = out_gu;
+    VEXT_CUDA(cudaMemsetAsync(a.counts, 0, sizeof(int) * n_bins, st));
+    VEXT_CUDA(cudaMemsetAsync(a.cursor, 0, sizeof(int) * n_bins, st));
+    VEXT_CUDA(cudaMemsetAsync(d_refine, 0, sizeof(int), st));
+    const int pb = (n + 255) / 256;
+    pose_prep_kernel<<<pb, 256, 0, st>>>(a);
+    VEXT_CUDA(cudaGetLastError());
+    pose_scan_kernel<<<1, 1024, 0, st>>>(a);
+    VEXT_CUDA(cudaGetLastError());
+    pose_scatter_kernel<<<pb, 256, 0, st>>>(a);
+    VEXT_CUDA(cudaGetLastError());
+    const size_t smem = kStageBytes + (size_t)kCH * 4 * sizeof(double) + (size_t)a.n_types * 48;
+    VEXT_CUDA(cudaFuncSetAttribute(pose_kernel<kPoseThreads>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    pose_kernel<kPoseThreads><<<max_items, kPoseThreads, smem, st>>>(a);
+    VEXT_CUDA(cudaGetLastError());
+    if (refine) {
+        pose_refine_kernel<<<std::min(1184, (n + 7) / 8), 256, 0, st>>>(a);
+        VEXT_CUDA(cudaGetLastError());
+    }
+    if (host_io) {
+        if (energy)
+            VEXT_CUDA(cudaMemcpyAsync(energy, a.energy, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        if (gc)
+            VEXT_CUDA(cudaMemcpyAsync(gc, out_gc, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st));
+        if (gq)
+            VEXT_CUDA(cudaMemcpyAsync(gq, out_gq, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, st));
+        if (gu)
+            VEXT_CUDA(cudaMemcpyAsync(gu, out_gu, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st));
+    }
+    int status = 0;
+    VEXT_CUDA(cudaMemcpyAsync(&status, sys->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    VEXT_CUDA(cudaStreamSynchronize(st));
+    if (status) {
+        VEXT_CUDA(cudaMemsetAsync(sys->d_status, 0, sizeof(int), st));
+        VEXT_CUDA(cudaStreamSynchronize(st));
+        if (status == DEV_BAD_INPUT)
+            return fail(VEXT_ERR_ARGUMENT, "non-finite pose center or zero quaternion");
+        return fail(VEXT_ERR_TIMEOUT, "a device wait gave up (status %d)", status);
+    }
+    return 0;
+}
+
+}  // namespace vext
+
+using namespace vext;
+
+extern "C" int vext_pose_energy_grad(vext_system h, int n, const double *centers,
+                                     const double *quats, const vext_options *opt, double *energy,
+                                     double *grad_center, double *grad_quat,
+                                     double *grad_director) {
+    if (!h) return fail(VEXT_ERR_ARGUMENT, "null system");
+    System *sys = &h->sys;
+    std::lock_guard<std::mutex> guard(sys->lock);
+    VEXT_CUDA(cudaSetDevice(sys->device));
+    return pose_run(sys, n, centers, quats, resolve_options(opt), energy, grad_center, grad_quat,
+                    grad_director, sys->stream, true);
+}
+
+extern "C" int vext_pose_energy_grad_device(vext_system h, int n, const double *centers,
+                                            const double *quats, const vext_options *opt,
+                                            double *energy, double *grad_center,
+                                            double *grad_quat, double *grad_director,
+                                            void *stream) {
+    if (!h) return fail(VEXT_ERR_ARGUMENT, "null system");
+    System *sys = &h->sys;
+    std::lock_guard<std::mutex> guard(sys->lock);
+    VEXT_CUDA(cudaSetDevice(sys->device));
+    return pose_run(sys, n, centers, quats, resolve_options(opt), energy, grad_center, grad_quat,
+                    grad_director, (cudaStream_t)stream, false);
+}

@@ -1,0 +1,154 @@
+"""``VextSystem``: one framework + one symmetric two-site guest on the GPU.
+
+A thin owner of a ``vext_system`` handle (include/vext_b200.h).  All compute
+goes through the CUDA library; this class only marshals arrays.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .physics import body_offsets, require_identical_sites, validate_case
+
+
+def _c(a, dtype=np.float64):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+class VextSystem:
+    """Device-resident framework + guest.  ``case`` uses the reference's case
+    dictionary layout (src/string_vext/input.py:49-55)."""
+
+    def __init__(self, case: dict):
+        validate_case(case)
+        require_identical_sites(case)
+        self.case = case
+        self.cell = _c(case["cell"])
+        self.offsets = _c(body_offsets(case))
+        self._frac = _c(case["frame_frac"])
+        self._sigma = _c(case["frame_sigma"])
+        self._eps = _c(case["frame_epsilon"])
+        desc = _lib.SystemDesc()
+        desc.cell[:] = self.cell.reshape(-1).tolist()
+        desc.n_atoms = len(self._frac)
+        desc.frac = self._frac.ctypes.data
+        desc.sigma = self._sigma.ctypes.data
+        desc.epsilon = self._eps.ctypes.data
+        desc.guest_sigma = float(case["guest_sigma"][0])
+        desc.guest_epsilon = float(case["guest_epsilon"][0])
+        desc.offsets[:] = self.offsets.tolist()
+        desc.cutoff = float(case["cutoff"])
+        desc.temperature = float(case["temperature"])
+        handle = ctypes.c_void_p()
+        self._lib = _lib.load()
+        _lib.check(self._lib.vext_system_create(ctypes.byref(desc), ctypes.byref(handle)))
+        self.handle = handle
+        self.last_stats: dict | None = None
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self._lib.vext_system_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def invalidate(self) -> None:
+        """Drop cached region lists (the next call rebuilds them)."""
+        _lib.check(self._lib.vext_system_invalidate(self.handle))
+
+    def last_timings(self) -> dict:
+        """Device ms of the last list build, field kernel and epilogue."""
+        vals = [ctypes.c_double() for _ in range(3)]
+        _lib.check(self._lib.vext_last_timings(self.handle, *(ctypes.byref(v) for v in vals)))
+        return {"list_ms": vals[0].value, "kernel_ms": vals[1].value,
+                "epilogue_ms": vals[2].value}
+
+    def count_pairs(self, size: int, axes) -> int:
+        """Exact in-cutoff (site, image) pairs of the size^3 x len(axes) field."""
+        axes = _c(axes)
+        out = ctypes.c_int64()
+        _lib.check(self._lib.vext_count_pairs(self.handle, size, len(axes), _lib.ptr(axes),
+                                              ctypes.byref(out)))
+        return out.value
+
+    # ------------------------------------------------------------------ field
+    def field(self, size: int, axes, mode: int = _lib.VEXT_MODE_MIXED,
+              orientation: bool = True, energy: bool = False, marginal: bool = False,
+              site: bool = False, grid: bool = False, **opts) -> dict:
+        """Vext field on the size^3 grid x unit directors ``axes`` (host arrays).
+        Returns the requested channels in the reference layout."""
+        axes = _c(axes)
+        n_axes = len(axes)
+        s3 = size ** 3
+        out = {}
+        o_k = np.empty((n_axes, size, size, size), np.float32) if orientation else None
+        e64 = np.empty((s3, n_axes), np.float64) if energy else None
+        m_k = np.empty((size, size, size), np.float32) if marginal else None
+        s_k = np.empty((2, size, size, size), np.float32) if site else None
+        g_k = np.empty((size, size, size), np.float32) if grid else None
+        stats = _lib.FieldStats()
+        opt = _lib.options(mode, **opts)
+        _lib.check(self._lib.vext_field(self.handle, size, n_axes, _lib.ptr(axes),
+                                        ctypes.byref(opt), _lib.ptr(o_k), _lib.ptr(e64),
+                                        _lib.ptr(m_k), _lib.ptr(s_k), _lib.ptr(g_k),
+                                        ctypes.byref(stats)))
+        self.last_stats = stats.as_dict()
+        for key, value in (("orientation_K", o_k), ("energy", e64), ("marginal_K", m_k),
+                           ("site_K", s_k), ("grid", g_k)):
+            if value is not None:
+                out[key] = value
+        return out
+
+    def field_device(self, size: int, axes, out_orientation, mode: int = _lib.VEXT_MODE_MIXED,
+                     out_energy=None, out_marginal=None, out_site=None, out_grid=None,
+                     stream=None, **opts) -> None:
+        """Device-pointer variant: outputs are CUDA tensors (float32 [O, S, S, S]
+        etc.), work is enqueued on ``stream`` (a torch.cuda.Stream or None)."""
+        axes = _c(axes)
+        opt = _lib.options(mode, **opts)
+        handle = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        _lib.check(self._lib.vext_field_device(self.handle, size, len(axes), _lib.ptr(axes),
+                                               ctypes.byref(opt), _lib.ptr(out_orientation),
+                                               _lib.ptr(out_energy), _lib.ptr(out_marginal),
+                                               _lib.ptr(out_site), _lib.ptr(out_grid), handle))
+
+    # ------------------------------------------------------------------ poses
+    def pose_energy_grad(self, centers, quats, mode: int = _lib.VEXT_MODE_MIXED,
+                         grad: bool = True, **opts):
+        """Host arrays: centers (n, 3) Cartesian A, quats (n, 4) (w, x, y, z).
+        Returns energy (n,), dE/dcenter (n, 3), dE/dq (n, 4), dE/du (n, 3)."""
+        centers, quats = _c(centers), _c(quats)
+        n = len(centers)
+        e = np.empty(n)
+        gc = np.empty((n, 3)) if grad else None
+        gq = np.empty((n, 4)) if grad else None
+        gu = np.empty((n, 3)) if grad else None
+        opt = _lib.options(mode, **opts)
+        _lib.check(self._lib.vext_pose_energy_grad(self.handle, n, _lib.ptr(centers),
+                                                   _lib.ptr(quats), ctypes.byref(opt),
+                                                   _lib.ptr(e), _lib.ptr(gc), _lib.ptr(gq),
+                                                   _lib.ptr(gu)))
+        return e, gc, gq, gu
+
+    def pose_energy_grad_device(self, centers, quats, energy, grad_center=None, grad_quat=None,
+                                grad_director=None, mode: int = _lib.VEXT_MODE_MIXED,
+                                stream=None, **opts) -> None:
+        """CUDA float64 tensors in and out, enqueued on ``stream``."""
+        opt = _lib.options(mode, **opts)
+        handle = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        _lib.check(self._lib.vext_pose_energy_grad_device(
+            self.handle, int(centers.shape[0]), _lib.ptr(centers), _lib.ptr(quats),
+            ctypes.byref(opt), _lib.ptr(energy), _lib.ptr(grad_center), _lib.ptr(grad_quat),
+            _lib.ptr(grad_director), handle))

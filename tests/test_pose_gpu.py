@@ -1,0 +1,153 @@
+"""Pose energies and the hand-written adjoint through the C ABI: against the
+FP64 oracle's analytic gradient, FP64 central differences, and the
+reference String solver's forward-difference forces (restated in the
+oracle, global.h:1141-1325); the torch autograd Function."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle
+from string_vext_b200 import _lib, synth
+from string_vext_b200.autograd import pose_energy
+from string_vext_b200.system import VextSystem
+
+pytestmark = pytest.mark.gpu
+
+FP64 = _lib.VEXT_MODE_FP64
+MIXED = _lib.VEXT_MODE_MIXED
+
+
+def director(q):
+    q = q / np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    return np.stack([1 - 2 * (y * y + z * z), 2 * (x * y + w * z), 2 * (x * z - w * y)], 1)
+
+
+def random_poses(case, n, seed):
+    rng = np.random.default_rng(seed)
+    frac = rng.random((n, 3))
+    q = rng.normal(size=(n, 4))
+    return frac @ case["cell"], q / np.linalg.norm(q, axis=1, keepdims=True)
+
+
+@pytest.fixture(scope="module")
+def small():
+    case = synth.small_field()
+    with VextSystem(case) as system:
+        yield case, system
+
+
+def test_fp64_energy_and_gradient_match_oracle(small):
+    case, system = small
+    c, q = random_poses(case, 200, 11)
+    e, gc, gq, gu = system.pose_energy_grad(c, q, mode=FP64)
+    re, rgc, rgu = oracle.pose_energy_grad(case, c, director(q))
+    np.testing.assert_allclose(e, re, rtol=1e-10, atol=1e-8)
+    scale = np.maximum(np.abs(rgc).max(axis=1, keepdims=True), 1.0)
+    assert (np.abs(gc - rgc) / scale).max() < 1e-9
+    assert (np.abs(gu - rgu) / np.maximum(np.abs(rgu).max(axis=1, keepdims=True), 1.0)).max() < 1e-9
+
+
+def test_mixed_matches_fp64(small):
+    case, system = small
+    c, q = random_poses(case, 4096, 12)
+    e64, gc64, gq64, _ = system.pose_energy_grad(c, q, mode=FP64)
+    e, gc, gq, _ = system.pose_energy_grad(c, q, mode=MIXED)
+    neg = e64 <= 0
+    assert np.abs(e - e64)[neg].max() < 1e-4
+    assert (np.abs(e - e64) / np.maximum(np.abs(e64), 1))[~neg].max() < 1e-6
+    scale = np.maximum(np.abs(gc64).max(axis=1, keepdims=True), 1.0)
+    assert (np.abs(gc - gc64) / scale).max() < 1e-5
+
+
+def test_gradients_match_central_differences(small):
+    """dE/dcenter and dE/dq (tangent) vs FP64 central differences,
+    h = 1e-4 A and 1e-4 rad, on accessible poses."""
+    case, system = small
+    c, q = random_poses(case, 512, 13)
+    e, gc, gq, _ = system.pose_energy_grad(c, q, mode=FP64)
+    keep = e < 1e3
+    c, q, gc, gq = c[keep][:64], q[keep][:64], gc[keep][:64], gq[keep][:64]
+    h = 1e-4
+    for k in range(3):
+        d = np.zeros(3)
+        d[k] = h
+        ep, *_ = system.pose_energy_grad(c + d, q, mode=FP64, grad=False)
+        em, *_ = system.pose_energy_grad(c - d, q, mode=FP64, grad=False)
+        fd = (ep - em) / (2 * h)
+        np.testing.assert_allclose(gc[:, k], fd, rtol=1e-5, atol=1e-5 * np.abs(gc).max())
+    # rotate by a small angle t about lab axis e_k: q(t) = exp(t e_k / 2) q,
+    # a tangent direction with dq/dt = (0, e_k / 2) q at t = 0
+    def qmul(a, b):
+        w = a[..., 0] * b[..., 0] - (a[..., 1:] * b[..., 1:]).sum(-1)
+        v = (a[..., :1] * b[..., 1:] + b[..., :1] * a[..., 1:]
+             + np.cross(a[..., 1:], b[..., 1:]))
+        return np.concatenate([w[..., None], v], -1)
+
+    for k in range(3):
+        axis = np.zeros(3)
+        axis[k] = 1.0
+        rot = lambda t: qmul(np.r_[np.cos(t / 2), np.sin(t / 2) * axis][None], q)
+        ep, *_ = system.pose_energy_grad(c, rot(h), mode=FP64, grad=False)
+        em, *_ = system.pose_energy_grad(c, rot(-h), mode=FP64, grad=False)
+        fd = (ep - em) / (2 * h)
+        dq = qmul(np.r_[0.0, axis / 2][None], q)
+        np.testing.assert_allclose((gq * dq).sum(1), fd, rtol=1e-5, atol=1e-5 * np.abs(fd).max())
+
+
+def test_against_reference_string_forces(small):
+    """The reference's String 'forces' are one-sided differences over
+    (frac a, b, c, Euler alpha, beta, gamma), not divided by the step.  With
+    small steps they equal step x the analytic gradient in those coordinates."""
+    case, system = small
+    rng = np.random.default_rng(14)
+    poses = np.column_stack([rng.random((24, 3)), rng.uniform(-np.pi, np.pi, (24, 3))])
+    hf, ha = 1e-7, 1e-7
+    ref = oracle.string_fd_gradient(case, poses, delta_frac=hf, delta_angle_rad=ha,
+                                    rounding=1e-30)
+    a, b, g = poses[:, 3], poses[:, 4], poses[:, 5]
+    u = np.stack([np.cos(g) * np.cos(b), np.sin(g) * np.cos(b), -np.sin(b)], 1)
+    # quaternion of R = Rz(g) Ry(b) Rx(a)
+    ca, sa, cb, sb, cg, sg = (np.cos(a / 2), np.sin(a / 2), np.cos(b / 2), np.sin(b / 2),
+                              np.cos(g / 2), np.sin(g / 2))
+    quat = np.stack([cg * cb * ca + sg * sb * sa, cg * cb * sa - sg * sb * ca,
+                     cg * sb * ca + sg * cb * sa, sg * cb * ca - cg * sb * sa], 1)
+    np.testing.assert_allclose(director(quat), u, atol=1e-12)
+    e, gc, _, gu = system.pose_energy_grad(poses[:, :3] @ case["cell"], quat, mode=FP64)
+    np.testing.assert_allclose(e, oracle.euler_pose_energy(case, poses), rtol=1e-10, atol=1e-8)
+    g_frac = gc @ case["cell"].T
+    du_db = np.stack([-np.cos(g) * np.sin(b), -np.sin(g) * np.sin(b), -np.cos(b)], 1)
+    du_dg = np.stack([-np.sin(g) * np.cos(b), np.cos(g) * np.cos(b), np.zeros_like(b)], 1)
+    analytic = np.column_stack([g_frac * hf, np.zeros(len(a)), (gu * du_db).sum(1) * ha,
+                                (gu * du_dg).sum(1) * ha])
+    scale = np.maximum(np.abs(analytic).max(axis=1, keepdims=True), 1e-9)
+    assert (np.abs(analytic - ref) / scale).max() < 1e-3
+
+
+def test_autograd_function(small):
+    case, system = small
+    c, q = random_poses(case, 256, 15)
+    ct = torch.tensor(c, device="cuda", requires_grad=True)
+    qt = torch.tensor(q, device="cuda", requires_grad=True)
+    e = pose_energy(system, ct, qt, _lib.VEXT_MODE_FP64)
+    weights = torch.linspace(0.5, 1.5, len(c), device="cuda", dtype=torch.float64)
+    (e * weights).sum().backward()
+    e_np, gc, gq, _ = system.pose_energy_grad(c, q, mode=FP64)
+    np.testing.assert_allclose(e.detach().cpu().numpy(), e_np, rtol=0, atol=0)
+    w = weights.cpu().numpy()[:, None]
+    np.testing.assert_allclose(ct.grad.cpu().numpy(), w * gc, rtol=1e-14, atol=0)
+    np.testing.assert_allclose(qt.grad.cpu().numpy(), w * gq, rtol=1e-14, atol=0)
+
+
+def test_string_path_and_random_batch():
+    case, pf, pq, bf, bq = synth.string_path()
+    with VextSystem(case) as system:
+        for frac, quat in ((pf, pq), (bf[:8192], bq[:8192])):
+            cart = frac @ case["cell"]
+            e64, gc64, *_ = system.pose_energy_grad(cart, quat, mode=FP64)
+            e, gc, *_ = system.pose_energy_grad(cart, quat, mode=MIXED)
+            neg = e64 <= 0
+            assert np.abs(e - e64)[neg].max(initial=0) < 1e-4
+            assert (np.abs(e - e64) / np.maximum(np.abs(e64), 1))[~neg].max(initial=0) < 1e-6
+            ref = oracle.pose_energy_grad(case, cart[:64], director(quat[:64]))[0]
+            np.testing.assert_allclose(e64[:64], ref, rtol=1e-10, atol=1e-8)
