@@ -308,7 +308,7 @@ def run_ours(args, rank, world, local_rank):
     line = {"metric": METRIC, "value": value, "unit": "poses/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32+f64 (FP64 pairs < 8 A, FP32 beyond, FP64 refinement)",
+            "dtype": "f32+f64 (FP64 pairs < 6 A, FP32 beyond, FP64 refinement)",
             "data": "synthetic", "config": config_of(args.workload, size),
             "e2e": {"value": e2e_value, "unit": "poses/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "path": "vext_system_create + vext_field "

@@ -24,7 +24,7 @@
 namespace vext {
 
 constexpr int kMaxTypes = 1024;     // distinct framework (sigma, epsilon) pairs
-constexpr double kDefaultRSplit = 8.0;
+constexpr double kDefaultRSplit = 6.0;
 
 struct alignas(16) RegionInfo {
     double of[3];       // origin, fractional

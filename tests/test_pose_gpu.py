@@ -101,10 +101,13 @@ def test_against_reference_string_forces(small):
     small steps they equal step x the analytic gradient in those coordinates."""
     case, system = small
     rng = np.random.default_rng(14)
-    poses = np.column_stack([rng.random((24, 3)), rng.uniform(-np.pi, np.pi, (24, 3))])
+    poses = np.column_stack([rng.random((3000, 3)), rng.uniform(-np.pi, np.pi, (3000, 3))])
+    # String images are accessible poses; keep those (E < 1e4 K)
+    poses = poses[oracle.euler_pose_energy(case, poses) < 1e4][:24]
+    assert len(poses) >= 12
     hf, ha = 1e-7, 1e-7
     ref = oracle.string_fd_gradient(case, poses, delta_frac=hf, delta_angle_rad=ha,
-                                    rounding=1e-30)
+                                    rounding=1e-15)
     a, b, g = poses[:, 3], poses[:, 4], poses[:, 5]
     u = np.stack([np.cos(g) * np.cos(b), np.sin(g) * np.cos(b), -np.sin(b)], 1)
     # quaternion of R = Rz(g) Ry(b) Rx(a)
@@ -121,7 +124,7 @@ def test_against_reference_string_forces(small):
     analytic = np.column_stack([g_frac * hf, np.zeros(len(a)), (gu * du_db).sum(1) * ha,
                                 (gu * du_dg).sum(1) * ha])
     scale = np.maximum(np.abs(analytic).max(axis=1, keepdims=True), 1e-9)
-    assert (np.abs(analytic - ref) / scale).max() < 1e-3
+    assert (np.abs(analytic - ref) / scale).max() < 1e-4
 
 
 def test_autograd_function(small):
