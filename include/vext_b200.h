@@ -60,6 +60,28 @@ VEXT_API int evaluate_reused_neighbors(int n_centers, int n_axes, int n_images, 
                               const double *shift, const double *floor2, const int64_t *starts,
                               const int32_t *indices, double *output);
 
+/* The same pair sum for callers that cannot allocate device memory: code
+ * running inside CUDA stream capture (where cudaMalloc is not allowed),
+ * plug-ins whose host runtime owns the GPU memory budget, real-time loops
+ * that cannot afford an allocation's synchronisation.  It has no counterpart
+ * in the reference.  Same arguments, host buffers, codes and bit-identical
+ * output as evaluate_reused_neighbors, but it calls no cudaMalloc/cudaFree/
+ * cudaMallocHost and uses no host heap: its scratch is one 64 MiB device
+ * array compiled into the library (held by every GPU that loads it until
+ * exit).  Batches needing more than 64 MiB of scratch (about 120 B per image +
+ * 4 B per neighbour index + 8 B per output pose) return VEXT_ERR_CAPACITY.
+ * The first call on each device resolves the array's address and loads its
+ * module, so make it before any stream capture.  Calls are serialised inside
+ * the process and finish before returning; the array keeps the last call's
+ * contents, and overlapping calls would race on it. */
+VEXT_API int evaluate_reused_neighbors_noalloc(int n_centers, int n_axes, int n_images,
+                                               double cutoff2, const double *centers,
+                                               const double *axes, const double *images,
+                                               const double *offsets, const double *coeff12,
+                                               const double *coeff6, const double *shift,
+                                               const double *floor2, const int64_t *starts,
+                                               const int32_t *indices, double *output);
+
 /* Message describing the calling thread's last nonzero status. */
 VEXT_API const char *vext_last_error(void);
 

@@ -69,6 +69,8 @@ def load() -> ctypes.CDLL:
     vp, ci, cd = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
     lib.evaluate_reused_neighbors.argtypes = [ci, ci, ci, cd] + [vp] * 11
     lib.evaluate_reused_neighbors.restype = ci
+    lib.evaluate_reused_neighbors_noalloc.argtypes = [ci, ci, ci, cd] + [vp] * 11
+    lib.evaluate_reused_neighbors_noalloc.restype = ci
     lib.vext_last_error.argtypes = []
     lib.vext_last_error.restype = ctypes.c_char_p
     lib.vext_version.argtypes = []
