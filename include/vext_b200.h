@@ -115,19 +115,22 @@ VEXT_API int vext_system_destroy(vext_system sys);
  * it (into the same device allocation when it still fits). */
 VEXT_API int vext_system_invalidate(vext_system sys);
 
-/* Device times (CUDA events on the launching stream) of the system's most
- * recent list build and of the most recent field call's main kernel and
- * epilogue, in ms; waits for those events.  list_ms is 0 if no list was
- * built since the previous query. */
-VEXT_API int vext_last_timings(vext_system sys, double *list_ms, double *kernel_ms,
-                               double *epilogue_ms);
+/* Device times (CUDA events on the launching stream), in ms, of the
+ * system's most recent list build and of the most recent field call's near
+ * (FP64) pair kernel, far (FP32) pair kernel and epilogue; waits for those
+ * events.  list_ms is 0 if no list was built since the previous query; in
+ * the FP64 modes near_ms is the whole pair kernel and far_ms 0. */
+VEXT_API int vext_last_timings(vext_system sys, double *list_ms, double *near_ms,
+                               double *far_ms, double *epilogue_ms);
 
 /* Precision modes. */
 enum {
     VEXT_MODE_MIXED = 0,     /* FP64 for pairs nearer than r_split, FP32 beyond,
                                 FP64 re-evaluation of poses whose energy lies in
                                 the refinement band                           */
-    VEXT_MODE_FP64 = 1       /* every pair in FP64 (the GPU oracle kernel)     */
+    VEXT_MODE_FP64 = 1,      /* every pair in FP64 (the GPU oracle kernel)     */
+    VEXT_MODE_FP64_PLAIN = 2 /* fields only: the plain FP64 baseline kernel
+                                (one thread per pose, no staging)            */
 };
 
 typedef struct {
@@ -136,8 +139,9 @@ typedef struct {
     double band_lo, band_hi; /* refinement band for E (K); band_hi <= band_lo
                                 disables refinement; defaults via
                                 vext_default_options                          */
-    int centers_per_region;  /* 16 or 32; 0 = autotuned                       */
-    int reserved[4];
+    int centers_per_region;  /* 16 or 32; 0 = default (16)                    */
+    int variant;             /* pair-kernel shape; 0 = default                */
+    int reserved[3];
 } vext_options;
 
 VEXT_API void vext_default_options(vext_options *opt);
@@ -204,10 +208,18 @@ VEXT_API int vext_pose_energy_grad_device(vext_system sys, int n, const double *
  * the run length. */
 VEXT_API int vext_measure_fp32_peak(int iterations, double *flops_per_second);
 
+/* Measured throughput of the SIMT pipes the pair kernels use: scalar FFMA
+ * (FMA/s), packed FFMA2 (FMA/s, two per lane per instruction) and the
+ * hardware reciprocal (results/s); any pointer may be NULL. */
+VEXT_API int vext_measure_pipes(int iterations, double *ffma_per_s, double *ffma2_fma_per_s,
+                                double *rcp_per_s);
+
 /* Exact FP64 number of (site, image) pairs closer than the cutoff over the
- * size^3 x n_axes field (the algorithmic unit of work). */
+ * size^3 x n_axes field (the algorithmic unit of work); far_pairs (may be
+ * NULL) receives those whose image is a far entry for the given r_split
+ * (<= 0: the default), i.e. the pairs the FP32 far kernel evaluates. */
 VEXT_API int vext_count_pairs(vext_system sys, int size, int n_axes, const double *axes,
-                              int64_t *pairs);
+                              double r_split, int64_t *pairs, int64_t *far_pairs);
 
 /* Library version string. */
 VEXT_API const char *vext_version(void);

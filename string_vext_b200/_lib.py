@@ -18,6 +18,7 @@ LIB_PATH = Path(os.environ.get("VEXT_B200_LIBRARY", PACKAGE / "lib" / "libvext_b
 
 VEXT_MODE_MIXED = 0
 VEXT_MODE_FP64 = 1
+VEXT_MODE_FP64_PLAIN = 2
 
 STATUS = {0: "ok", 1: "bad sizes", 2: "CSR starts decreasing", 3: "CSR index out of range",
           4: "non-finite energy", 16: "CUDA error", 17: "device wait timeout",
@@ -35,7 +36,8 @@ class SystemDesc(ctypes.Structure):
 class Options(ctypes.Structure):
     _fields_ = [("mode", ctypes.c_int), ("r_split", ctypes.c_double),
                 ("band_lo", ctypes.c_double), ("band_hi", ctypes.c_double),
-                ("centers_per_region", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
+                ("centers_per_region", ctypes.c_int), ("variant", ctypes.c_int),
+                ("reserved", ctypes.c_int * 3)]
 
 
 class FieldStats(ctypes.Structure):
@@ -94,10 +96,13 @@ def load() -> ctypes.CDLL:
     lib.vext_pose_energy_grad_device.restype = ci
     lib.vext_system_invalidate.argtypes = [vp]
     lib.vext_system_invalidate.restype = ci
-    lib.vext_last_timings.argtypes = [vp] + [ctypes.POINTER(ctypes.c_double)] * 3
+    lib.vext_last_timings.argtypes = [vp] + [ctypes.POINTER(ctypes.c_double)] * 4
     lib.vext_last_timings.restype = ci
-    lib.vext_count_pairs.argtypes = [vp, ci, ci, vp, ctypes.POINTER(ctypes.c_int64)]
+    lib.vext_count_pairs.argtypes = [vp, ci, ci, vp, cd, ctypes.POINTER(ctypes.c_int64),
+                                     ctypes.POINTER(ctypes.c_int64)]
     lib.vext_count_pairs.restype = ci
+    lib.vext_measure_pipes.argtypes = [ci] + [ctypes.POINTER(ctypes.c_double)] * 3
+    lib.vext_measure_pipes.restype = ci
     lib.vext_measure_fp32_peak.argtypes = [ci, ctypes.POINTER(ctypes.c_double)]
     lib.vext_measure_fp32_peak.restype = ci
     _lib = lib
@@ -121,7 +126,7 @@ def ptr(array) -> ctypes.c_void_p | None:
 
 def options(mode: int = VEXT_MODE_MIXED, r_split: float | None = None,
             band: tuple[float, float] | None = None,
-            centers_per_region: int | None = None) -> Options:
+            centers_per_region: int | None = None, variant: int | None = None) -> Options:
     opt = Options()
     load().vext_default_options(ctypes.byref(opt))
     opt.mode = mode
@@ -131,6 +136,8 @@ def options(mode: int = VEXT_MODE_MIXED, r_split: float | None = None,
         opt.band_lo, opt.band_hi = band
     if centers_per_region is not None:
         opt.centers_per_region = centers_per_region
+    if variant is not None:
+        opt.variant = variant
     return opt
 
 
@@ -142,3 +149,11 @@ def measure_fp32_peak(iterations: int = 20000) -> float:
     value = ctypes.c_double()
     check(load().vext_measure_fp32_peak(iterations, ctypes.byref(value)))
     return value.value
+
+
+def measure_pipes(iterations: int = 20000) -> dict:
+    """FFMA, FFMA2 (counted per FMA) and RCP throughput of the current GPU."""
+    vals = [ctypes.c_double() for _ in range(3)]
+    check(load().vext_measure_pipes(iterations, *(ctypes.byref(v) for v in vals)))
+    return {"ffma_per_s": vals[0].value, "ffma2_fma_per_s": vals[1].value,
+            "rcp_per_s": vals[2].value}

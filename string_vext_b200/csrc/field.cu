@@ -25,6 +25,8 @@
 
 namespace vext {
 
+constexpr int kPlainVariant = 1 << 20;
+
 struct FieldArgs {
     Mat3 H;
     double rc2;
@@ -40,6 +42,7 @@ struct FieldArgs {
     const double *td;
     int n_types;
     double *e64;              // [O][S^3]
+    double *e64b;             // far sums go here instead of into e64 when non-null
     int *status;
 };
 
@@ -51,8 +54,72 @@ __device__ __forceinline__ void center_of(const FieldArgs &a, const RegionInfo &
     gk = r.k0 + lk;
 }
 
-template <int CB, int G, int P>
-__global__ void __launch_bounds__(CB *G, 2) field_kernel(FieldArgs a) {
+// Shared set-up of both pair kernels: barriers, type tables, first copies.
+template <int NT>
+__device__ __forceinline__ void stage_begin(Stager &st, const ChunkPlan &plan, const FieldArgs &a,
+                                            float4 *stf, double *std4) {
+    const int tid = threadIdx.x;
+    for (int t = tid; t < a.n_types; t += NT) {
+        stf[t] = a.tf[t];
+        if (std4)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) std4[4 * t + k] = a.td[4 * t + k];
+    }
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) mbar_init(&st.bar[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int c = 0; c < min(kStages, plan.n_chunks); ++c) st.issue(plan, a.hi, a.lo, c, c);
+}
+
+// Wait for chunk c; on a failed wait drain the copies in flight and report
+// false (the whole CTA then returns).
+__device__ __forceinline__ bool stage_wait(Stager &st, const ChunkPlan &plan, int c, int *status) {
+    const bool ok = mbar_wait_bounded(&st.bar[c % kStages], (c / kStages) & 1, status);
+    if (__syncthreads_and(ok)) return true;
+    if (threadIdx.x == 0)
+        for (int cc = c; cc < min(c + kStages, plan.n_chunks); ++cc)
+            mbar_drain(&st.bar[cc % kStages], (cc / kStages) & 1);
+    return false;
+}
+
+__device__ __forceinline__ void stage_next(Stager &st, const ChunkPlan &plan, const FieldArgs &a,
+                                           int c) {
+    __syncthreads();
+    if (threadIdx.x == 0 && c + kStages < plan.n_chunks)
+        st.issue(plan, a.hi, a.lo, c + kStages, c + kStages);
+}
+
+
+__device__ __forceinline__ float set_lt(float a, float b) {
+    float r;
+    asm("set.lt.f32.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
+
+// FP64 reciprocal: hardware seed refined by two Newton-Raphson steps
+// r' = r + r (1 - s r).  Each step squares the relative error; one step
+// leaves a measurable one-sided (under-estimating) bias, two do not.
+__device__ __forceinline__ double rcp64_nr(double s) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(s));
+    r = fma(r, fma(-s, r, 1.0), r);
+    return fma(r, fma(-s, r, 1.0), r);
+}
+
+// Near pairs in FP64: E[pose] = sum over the region's near entries (all
+// entries for the FP64 oracle region set).
+//   MODE 0 (the FP64 oracle kernel): direct d = site - x per site, IEEE
+//          reciprocal, cutoff test.
+//   MODE 1/2 (mixed precision): every thread's poses share one grid center
+//          c, so with d0 = x - c, t = d0 . u:  q_s = |d0|^2 + o_s^2 - 2 o_s t
+//          (|d0|^2 once per entry, 1 FMA per site after t); Newton-refined
+//          reciprocal.  MODE 2 drops the cutoff test: near pairs are never
+//          farther apart than r_split + 2 rho_site < rc (checked on the host).
+template <int CB, int G, int P, int MODE>
+__global__ void __launch_bounds__(CB *G, 1) field_near_kernel(FieldArgs a) {
     constexpr int NT = CB * G;
     extern __shared__ __align__(128) unsigned char smem[];
     Stager st;
@@ -66,85 +133,59 @@ __global__ void __launch_bounds__(CB *G, 2) field_kernel(FieldArgs a) {
     const int tid = threadIdx.x;
     const RegionInfo r = a.regs[blockIdx.x];
     ChunkPlan plan;
-    plan.init(r);
+    plan.init_range(r.off, r.n_near, r.n_near);
+    stage_begin<NT>(st, plan, a, stf, std4);
 
-    for (int t = tid; t < a.n_types; t += NT) {
-        stf[t] = a.tf[t];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) std4[4 * t + k] = a.td[4 * t + k];
-    }
-    if (tid == 0) {
-        for (int s = 0; s < kStages; ++s) mbar_init(&st.bar[s], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-    if (tid == 0)
-        for (int c = 0; c < min(kStages, plan.n_chunks); ++c) st.issue(plan, a.hi, a.lo, c, c);
-
-    // ---- this thread's poses (FP64 set-up relative to the region origin)
     const int cl = tid % CB, og = tid / CB;
-    const int ncent = r.ni * r.nj * r.nk;
-    const bool cvalid = cl < ncent;
+    const bool cvalid = cl < r.ni * r.nj * r.nk;
     int gi, gj, gk;
     center_of(a, r, cvalid ? cl : 0, gi, gj, gk);
     double cx, cy, cz;
     frac_to_cart(a.H, (gi + .5) / a.S - r.of[0], (gj + .5) / a.S - r.of[1],
                  (gk + .5) / a.S - r.of[2], cx, cy, cz);
     const int obase = blockIdx.y * (G * P) + og;
-    double sd[P][2][3];
-    float sf[P][2][3];
+    double ux[P], uy[P], uz[P];
     double acc[P][2];
 #pragma unroll
     for (int p = 0; p < P; ++p) {
         const int o = min(obase + G * p, a.O - 1);
-        const double ux = a.axes[3 * o], uy = a.axes[3 * o + 1], uz = a.axes[3 * o + 2];
-#pragma unroll
-        for (int s = 0; s < 2; ++s) {
-            const double off = s ? a.off1 : a.off0;
-            sd[p][s][0] = cx + off * ux;
-            sd[p][s][1] = cy + off * uy;
-            sd[p][s][2] = cz + off * uz;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) sf[p][s][k] = (float)sd[p][s][k];
-            acc[p][s] = 0.0;
-        }
+        ux[p] = a.axes[3 * o];
+        uy[p] = a.axes[3 * o + 1];
+        uz[p] = a.axes[3 * o + 2];
+        acc[p][0] = acc[p][1] = 0.0;
     }
-
+    const double m0 = -2.0 * a.off0, m1 = -2.0 * a.off1;
+    const double oo0 = a.off0 * a.off0, oo1 = a.off1 * a.off1;
     for (int c = 0; c < plan.n_chunks; ++c) {
-        const int s = c % kStages;
-        const bool ok = mbar_wait_bounded(&st.bar[s], (c / kStages) & 1, a.status);
-        if (!__syncthreads_and(ok)) {
-            if (tid == 0)   // let copies already in flight land before exiting
-                for (int cc = c; cc < min(c + kStages, plan.n_chunks); ++cc)
-                    mbar_drain(&st.bar[cc % kStages], (cc / kStages) & 1);
-            return;
-        }
+        if (!stage_wait(st, plan, c, a.status)) return;
         int start, len;
         bool near;
         plan.chunk(c, start, len, near);
-        if (near) {
-            const float4 *hb = st.hib + s * kCH, *lb = st.lob + s * kCH;
-            for (int e = tid; e < len; e += NT) {
-                const float4 h = hb[e], l = lb[e];
-                ed[4 * e + 0] = (double)h.x + (double)l.x;
-                ed[4 * e + 1] = (double)h.y + (double)l.y;
-                ed[4 * e + 2] = (double)h.z + (double)l.z;
-                ed[4 * e + 3] = (double)__float_as_int(h.w);
-            }
-            __syncthreads();
-            const double2 *ed2 = reinterpret_cast<const double2 *>(ed);
-            const double2 *td2 = reinterpret_cast<const double2 *>(std4);
+        const int s = c % kStages;
+        const float4 *hb = st.hib + s * kCH, *lb = st.lob + s * kCH;
+        for (int e = tid; e < len; e += NT) {
+            const float4 h = hb[e], l = lb[e];
+            ed[4 * e + 0] = (double)h.x + (double)l.x;
+            ed[4 * e + 1] = (double)h.y + (double)l.y;
+            ed[4 * e + 2] = (double)h.z + (double)l.z;
+            ed[4 * e + 3] = (double)__float_as_int(h.w);
+        }
+        __syncthreads();
+        const double2 *ed2 = reinterpret_cast<const double2 *>(ed);
+        const double2 *td2 = reinterpret_cast<const double2 *>(std4);
 #pragma unroll 1
-            for (int e = 0; e < len; ++e) {
-                const double2 xy = ed2[2 * e], zt = ed2[2 * e + 1];
-                const int t = (int)zt.y;
-                const double2 cc = td2[2 * t], sh = td2[2 * t + 1];   // (c12, c6), (shift, floor2)
+        for (int e = 0; e < len; ++e) {
+            const double2 xy = ed2[2 * e], zt = ed2[2 * e + 1];
+            const int t = (int)zt.y;
+            const double2 cc = td2[2 * t], sh = td2[2 * t + 1];   // (c12, c6), (shift, floor2)
+            if (MODE == 0) {
 #pragma unroll
                 for (int p = 0; p < P; ++p)
 #pragma unroll
                     for (int q = 0; q < 2; ++q) {
-                        const double dx = sd[p][q][0] - xy.x, dy = sd[p][q][1] - xy.y,
-                                     dz = sd[p][q][2] - zt.x;
+                        const double off = q ? a.off1 : a.off0;
+                        const double dx = cx + off * ux[p] - xy.x, dy = cy + off * uy[p] - xy.y,
+                                     dz = cz + off * uz[p] - zt.x;
                         const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
                         const double s2 = fmax(d2, sh.y);
                         const double i2 = __drcp_rn(s2);
@@ -152,45 +193,28 @@ __global__ void __launch_bounds__(CB *G, 2) field_kernel(FieldArgs a) {
                         const double en = fma(i6, fma(cc.x, i6, -cc.y), sh.x);
                         acc[p][q] += d2 < a.rc2 ? en : 0.0;
                     }
-            }
-        } else {
-            const float4 *hb = st.hib + s * kCH;
-#pragma unroll 1
-            for (int e0 = 0; e0 < len; e0 += 16) {
-                float fa[P][2];
-#pragma unroll
-                for (int p = 0; p < P; ++p) fa[p][0] = fa[p][1] = 0.f;
-                const int e1 = min(e0 + 16, len);
-#pragma unroll 2
-                for (int e = e0; e < e1; ++e) {
-                    const float4 h = hb[e];
-                    const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, floor2)
-#pragma unroll
-                    for (int p = 0; p < P; ++p)
-#pragma unroll
-                        for (int q = 0; q < 2; ++q) {
-                            const float dx = sf[p][q][0] - h.x, dy = sf[p][q][1] - h.y,
-                                        dz = sf[p][q][2] - h.z;
-                            const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                            const float s2 = fmaxf(d2, tp.w);
-                            const float i2 = rcp_nr(s2);
-                            const float i6 = i2 * i2 * i2;
-                            const float en = fmaf(i6, fmaf(tp.x, i6, -tp.y), tp.z);
-                            fa[p][q] += d2 < a.rc2f ? en : 0.f;
-                        }
-                }
+            } else {
+                const double dx = xy.x - cx, dy = xy.y - cy, dz = zt.x - cz;
+                const double dd = fma(dx, dx, fma(dy, dy, dz * dz));
+                const double k0 = dd + oo0, k1 = dd + oo1;
 #pragma unroll
                 for (int p = 0; p < P; ++p) {
-                    acc[p][0] += (double)fa[p][0];
-                    acc[p][1] += (double)fa[p][1];
+                    const double tt = fma(dx, ux[p], fma(dy, uy[p], dz * uz[p]));
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const double d2 = fma(q ? m1 : m0, tt, q ? k1 : k0);
+                        const double s2 = fmax(d2, sh.y);
+                        const double i2 = rcp64_nr(s2);
+                        const double i6 = i2 * i2 * i2;
+                        const double en = fma(i6, fma(cc.x, i6, -cc.y), sh.x);
+                        if (MODE == 1) acc[p][q] += d2 < a.rc2 ? en : 0.0;
+                        else acc[p][q] += en;
+                    }
                 }
             }
         }
-        __syncthreads();
-        if (tid == 0 && c + kStages < plan.n_chunks)
-            st.issue(plan, a.hi, a.lo, c + kStages, c + kStages);
+        stage_next(st, plan, a, c);
     }
-
     if (cvalid) {
         const size_t S3 = (size_t)a.S * a.S * a.S;
         const size_t cg = ((size_t)gi * a.S + gj) * a.S + gk;
@@ -199,6 +223,131 @@ __global__ void __launch_bounds__(CB *G, 2) field_kernel(FieldArgs a) {
             const int o = obase + G * p;
             if (o < a.O) a.e64[(size_t)o * S3 + cg] = acc[p][0] + acc[p][1];
         }
+    }
+}
+
+// Far pairs in packed FP32x2.  A thread owns one grid center c and P
+// directors; lanes .x/.y of a float2 hold two directors (p, p + 1).  Per
+// staged entry x (image relative to the region origin):
+//   d0 = x - c, D = |d0|^2 (scalar, once per entry; with CLO corrected by
+//        -2 d0 . c_lo, c_lo the FP32 rounding residual of the center),
+//   t = d0 . u  (packed over two directors),
+//   q_s = (D + o_s^2) - 2 o_s t  = |x - (c + o_s u)|^2  for site s;
+//   one hardware reciprocal per two pairs: nr = 1/(-q.x q.y),
+//   n = (q.y nr, q.x nr) = -1/q, refined by one Newton step n' = n + n(1 + q n);
+//   n3 = n'^3 = -1/q^3, e = n3 (c12 n3 + c6) + shift = c12/q^6 - c6/q^3 + shift;
+//   a 1/0 mask (q < rc^2) multiplies e into the FP32 partial sums, flushed
+//   into FP64 every 16 entries.
+// Far entries are >= r_split from every site, so no pair reaches the contact
+// floor.  The far sums are added into e64 (written by the near kernel) or
+// stored into e64b.
+template <int CB, int G, int P, int MINB, bool NEWTON = true, int FLUSH = 16, bool CLO = false>
+__global__ void __launch_bounds__(CB *G, MINB) field_far_kernel(FieldArgs a) {
+    static_assert(P % 2 == 0, "directors are packed in pairs");
+    constexpr int NT = CB * G, PP = P / 2;
+    extern __shared__ __align__(128) unsigned char smem[];
+    Stager st;
+    st.bar = reinterpret_cast<uint64_t *>(smem);
+    st.hib = reinterpret_cast<float4 *>(smem + 64);
+    st.lob = st.hib;   // far chunks bring hi only
+    float4 *stf = st.hib + kStages * kCH;
+
+    const int tid = threadIdx.x;
+    const RegionInfo r = a.regs[blockIdx.x];
+    ChunkPlan plan;
+    plan.init_range(r.off + r.n_near, 0, r.n_total - r.n_near);
+    stage_begin<NT>(st, plan, a, stf, nullptr);
+
+    const int cl = tid % CB, og = tid / CB;
+    const bool cvalid = cl < r.ni * r.nj * r.nk;
+    int gi, gj, gk;
+    center_of(a, r, cvalid ? cl : 0, gi, gj, gk);
+    double cxd, cyd, czd;
+    frac_to_cart(a.H, (gi + .5) / a.S - r.of[0], (gj + .5) / a.S - r.of[1],
+                 (gk + .5) / a.S - r.of[2], cxd, cyd, czd);
+    const float cx = (float)cxd, cy = (float)cyd, cz = (float)czd;
+    // FP32 residual of the center (used by the CLO variant: it removes the
+    // coherent displacement grad(E) . dc that rounding c gives every far pair
+    // of this thread, to first order in |x - c|^2).
+    const float cxl = (float)(cxd - cx), cyl = (float)(cyd - cy), czl = (float)(czd - cz);
+    const int obase = blockIdx.y * (G * P) + og;
+    float2 ux[PP], uy[PP], uz[PP];
+    double acc[P];
+#pragma unroll
+    for (int j = 0; j < PP; ++j) {
+        const int o0 = min(obase + G * (2 * j), a.O - 1), o1 = min(obase + G * (2 * j + 1), a.O - 1);
+        ux[j] = make_float2((float)a.axes[3 * o0], (float)a.axes[3 * o1]);
+        uy[j] = make_float2((float)a.axes[3 * o0 + 1], (float)a.axes[3 * o1 + 1]);
+        uz[j] = make_float2((float)a.axes[3 * o0 + 2], (float)a.axes[3 * o1 + 2]);
+        acc[2 * j] = acc[2 * j + 1] = 0.0;
+    }
+    const float2 m0 = make_float2(-2.f * (float)a.off0, -2.f * (float)a.off0);
+    const float2 m1 = make_float2(-2.f * (float)a.off1, -2.f * (float)a.off1);
+    const float oo0 = (float)(a.off0 * a.off0), oo1 = (float)(a.off1 * a.off1);
+    const float2 one2 = make_float2(1.f, 1.f);
+    const float rc2f = a.rc2f;
+    for (int c = 0; c < plan.n_chunks; ++c) {
+        if (!stage_wait(st, plan, c, a.status)) return;
+        int start, len;
+        bool near;
+        plan.chunk(c, start, len, near);
+        const float4 *hb = st.hib + (c % kStages) * kCH;
+#pragma unroll 1
+        for (int e0 = 0; e0 < len; e0 += FLUSH) {
+            float2 fa[PP];
+#pragma unroll
+            for (int j = 0; j < PP; ++j) fa[j] = make_float2(0.f, 0.f);
+            const int e1 = min(e0 + FLUSH, len);
+#pragma unroll 2
+            for (int e = e0; e < e1; ++e) {
+                const float4 h = hb[e];
+                const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, floor2)
+                const float dx = h.x - cx, dy = h.y - cy, dz = h.z - cz;
+                float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                if (CLO) dd = fmaf(-2.f, fmaf(dx, cxl, fmaf(dy, cyl, dz * czl)), dd);
+                const float2 k0 = make_float2(dd + oo0, dd + oo0), k1 = make_float2(dd + oo1, dd + oo1);
+                const float2 dx2 = make_float2(dx, dx), dy2 = make_float2(dy, dy),
+                             dz2 = make_float2(dz, dz);
+                const float2 c12 = make_float2(tp.x, tp.x), c6 = make_float2(tp.y, tp.y),
+                             sh = make_float2(tp.z, tp.z);
+#pragma unroll
+                for (int j = 0; j < PP; ++j) {
+                    const float2 t = __ffma2_rn(dx2, ux[j], __ffma2_rn(dy2, uy[j], __fmul2_rn(dz2, uz[j])));
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const float2 d2 = __ffma2_rn(q ? m1 : m0, t, q ? k1 : k0);
+                        float nr;
+                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(nr) : "f"(-d2.x * d2.y));
+                        float2 n = make_float2(d2.y * nr, d2.x * nr);
+                        if (NEWTON) n = __ffma2_rn(n, __ffma2_rn(d2, n, one2), n);
+                        const float2 n3 = __fmul2_rn(__fmul2_rn(n, n), n);
+                        const float2 en = __ffma2_rn(n3, __ffma2_rn(c12, n3, c6), sh);
+                        const float2 m = make_float2(set_lt(d2.x, rc2f), set_lt(d2.y, rc2f));
+                        fa[j] = __ffma2_rn(en, m, fa[j]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < PP; ++j) {
+                acc[2 * j] += (double)fa[j].x;
+                acc[2 * j + 1] += (double)fa[j].y;
+            }
+        }
+        stage_next(st, plan, a, c);
+    }
+    if (cvalid) {
+        const size_t S3 = (size_t)a.S * a.S * a.S;
+        const size_t cg = ((size_t)gi * a.S + gj) * a.S + gk;
+#pragma unroll
+        for (int j = 0; j < PP; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int o = obase + G * (2 * j + h);
+                if (o < a.O) {
+                    double *dst = a.e64b ? a.e64b : a.e64;   // separate buffer when run concurrently
+                    dst[(size_t)o * S3 + cg] = (a.e64b ? 0.0 : dst[(size_t)o * S3 + cg]) + acc[2 * j + h];
+                }
+            }
     }
 }
 
@@ -342,7 +491,7 @@ __global__ void count_kernel(FieldArgs a, unsigned long long *total) {
     const int lane = threadIdx.x & 31;
     const long long S3 = (long long)a.S * a.S * a.S;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    unsigned long long mine = 0;
+    unsigned long long mine = 0, far = 0;
     for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < S3;
          c += nwarps) {
         const int gi = (int)(c / ((long long)a.S * a.S)), gj = (int)((c / a.S) % a.S),
@@ -361,31 +510,125 @@ __global__ void count_kernel(FieldArgs a, unsigned long long *total) {
                     const double off = s ? a.off1 : a.off0;
                     const double dx = cx + off * ux - x, dy = cy + off * uy - y,
                                  dz = cz + off * uz - z;
-                    mine += (dx * dx + dy * dy + dz * dz) < a.rc2;
+                    const bool in = (dx * dx + dy * dy + dz * dz) < a.rc2;
+                    mine += in;
+                    far += in && e >= r.n_near;
                 }
             }
         }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
-    if (lane == 0) atomicAdd(total, mine);
+    for (int o = 16; o > 0; o >>= 1) {
+        mine += __shfl_xor_sync(0xffffffffu, mine, o);
+        far += __shfl_xor_sync(0xffffffffu, far, o);
+    }
+    if (lane == 0) {
+        atomicAdd(total, mine);
+        atomicAdd(total + 1, far);
+    }
+}
+
+// The plain FP64 baseline: one thread per pose, both sites, every entry of
+// its region read straight from global memory (hi + lo), IEEE division, no
+// staging, no register blocking -- the straightforward one-field-per-launch
+// FP64 kernel the tiled kernels are measured against.
+__global__ void __launch_bounds__(256) plain_fp64_kernel(FieldArgs a) {
+    const long long S3 = (long long)a.S * a.S * a.S;
+    const long long n = S3 * a.O;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long c = idx % S3;   // consecutive threads: consecutive centers
+        const int o = (int)(idx / S3);
+        const int gi = (int)(c / ((long long)a.S * a.S)), gj = (int)((c / a.S) % a.S),
+                  gk = (int)(c % a.S);
+        const RegionInfo r = a.regs[region_of(a, gi, gj, gk)];
+        double cx, cy, cz;
+        frac_to_cart(a.H, (gi + .5) / a.S - r.of[0], (gj + .5) / a.S - r.of[1],
+                     (gk + .5) / a.S - r.of[2], cx, cy, cz);
+        const double ux = a.axes[3 * o], uy = a.axes[3 * o + 1], uz = a.axes[3 * o + 2];
+        double e = 0.0;
+        for (int s = 0; s < 2; ++s) {
+            const double off = s ? a.off1 : a.off0;
+            const double px = cx + off * ux, py = cy + off * uy, pz = cz + off * uz;
+            for (int k = 0; k < r.n_total; ++k) {
+                const float4 h = a.hi[r.off + k], l = a.lo[r.off + k];
+                const double dx = px - ((double)h.x + (double)l.x);
+                const double dy = py - ((double)h.y + (double)l.y);
+                const double dz = pz - ((double)h.z + (double)l.z);
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                if (d2 >= a.rc2) continue;
+                const int t = __float_as_int(h.w);
+                const double fl = a.td[4 * t + 3];
+                const double s2 = d2 < fl ? fl : d2;
+                const double i2 = 1.0 / s2;
+                const double i6 = i2 * i2 * i2;
+                e += a.td[4 * t] * i6 * i6 - a.td[4 * t + 1] * i6 + a.td[4 * t + 2];
+            }
+        }
+        a.e64[idx] = e;
+    }
 }
 
 // ---------------------------------------------------------------- launchers
 
-static size_t field_smem(int n_types) {
+static size_t near_smem(int n_types) {
     return kStageBytes + (size_t)kCH * 4 * sizeof(double) + (size_t)n_types * (16 + 32);
 }
 
-template <int CB, int G, int P>
-static int launch_field_t(const FieldArgs &a, cudaStream_t stream) {
-    const size_t smem = field_smem(a.n_types);
-    auto kern = field_kernel<CB, G, P>;
+static size_t far_smem(int n_types) {
+    return 64 + (size_t)kStages * kCH * sizeof(float4) + (size_t)n_types * 16;
+}
+
+template <typename K>
+static int launch_t(K kern, dim3 grid, int threads, size_t smem, const FieldArgs &a,
+                    cudaStream_t stream) {
     VEXT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid(a.n_regions, (a.O + G * P - 1) / (G * P));
-    kern<<<grid, CB * G, smem, stream>>>(a);
+    kern<<<grid, threads, smem, stream>>>(a);
     VEXT_CUDA(cudaGetLastError());
     return 0;
+}
+
+// Near (FP64) kernel over every region.  mode 0 = the FP64 oracle kernel
+// (must run on an all-near region set), 1 = mixed with cutoff test, 2 =
+// mixed without (near pairs provably inside the cutoff).
+static int launch_near(const FieldArgs &a, int cb, int mode, cudaStream_t stream) {
+    const size_t smem = near_smem(a.n_types);
+    if (cb == 32) {
+        dim3 grid(a.n_regions, (a.O + 31) / 32);
+        if (mode == 0) return launch_t(field_near_kernel<32, 8, 4, 0>, grid, 256, smem, a, stream);
+        if (mode == 1) return launch_t(field_near_kernel<32, 8, 4, 1>, grid, 256, smem, a, stream);
+        return launch_t(field_near_kernel<32, 8, 4, 2>, grid, 256, smem, a, stream);
+    }
+    dim3 grid(a.n_regions, (a.O + 63) / 64);
+    if (mode == 0) return launch_t(field_near_kernel<16, 16, 4, 0>, grid, 256, smem, a, stream);
+    if (mode == 1) return launch_t(field_near_kernel<16, 16, 4, 1>, grid, 256, smem, a, stream);
+    return launch_t(field_near_kernel<16, 16, 4, 2>, grid, 256, smem, a, stream);
+}
+
+// Far-kernel variants (threads = CB x G, directors per CTA = G x P):
+//   0/5 (default): <16, 8, 4>, 4 CTAs/SM of 128      1: <16, 16, 4>, 2 CTAs/SM
+//   2: <16, 32, 2>, 1 CTA of 512/SM    3: <16, 16, 2>, 3 CTAs/SM
+//   4: <16, 16, 4>, 3 CTAs/SM
+// cb = 32 uses <32, 8, 4>.
+static int launch_far(const FieldArgs &a, int cb, int variant, cudaStream_t stream) {
+    const size_t smem = far_smem(a.n_types);
+    auto grid_for = [&](int per_cta) { return dim3(a.n_regions, (a.O + per_cta - 1) / per_cta); };
+    if (cb == 32) return launch_t(field_far_kernel<32, 8, 4, 2>, grid_for(32), 256, smem, a, stream);
+    if (variant & 32)   // without the Newton step (accuracy study)
+        return launch_t(field_far_kernel<16, 16, 4, 2, false>, grid_for(64), 256, smem, a, stream);
+    if (variant == 8)   // with the first-order centre-residual correction
+        return launch_t(field_far_kernel<16, 8, 4, 4, true, 16, true>, grid_for(32), 128, smem, a, stream);
+    if (variant & 64)   // FP32 partial sums flushed every 8 entries
+        return launch_t(field_far_kernel<16, 8, 4, 4, true, 8>, grid_for(32), 128, smem, a, stream);
+    if (variant & 128)  // ... every 4 entries
+        return launch_t(field_far_kernel<16, 8, 4, 4, true, 4>, grid_for(32), 128, smem, a, stream);
+    switch (variant) {
+    case 2: return launch_t(field_far_kernel<16, 32, 2, 1>, grid_for(64), 512, smem, a, stream);
+    case 3: return launch_t(field_far_kernel<16, 16, 2, 3>, grid_for(32), 256, smem, a, stream);
+    case 4: return launch_t(field_far_kernel<16, 16, 4, 3>, grid_for(64), 256, smem, a, stream);
+    case 1: return launch_t(field_far_kernel<16, 16, 4, 2>, grid_for(64), 256, smem, a, stream);
+    default: return launch_t(field_far_kernel<16, 8, 4, 4>, grid_for(32), 128, smem, a, stream);
+    }
 }
 
 static FieldArgs make_args(System *sys, const RegionSet *rs, int n_axes, const double *d_axes,
@@ -412,15 +655,56 @@ static FieldArgs make_args(System *sys, const RegionSet *rs, int n_axes, const d
     a.td = sys->d_td;
     a.n_types = sys->n_types;
     a.e64 = d_e64;
+    a.e64b = nullptr;
     a.status = sys->d_status;
     return a;
 }
 
+__global__ void add_kernel(double *dst, const double *src, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        dst[i] += src[i];
+}
+
+// variant & 16: near (FP64 pipe) and far (FP32 pipe) kernels on two streams
+// so their CTAs share the SMs; far sums land in a second buffer and are added
+// afterwards.  Otherwise the far kernel runs after the near one and adds in place.
 int launch_field(System *sys, const RegionSet *rs, int n_axes, const double *d_axes,
-                 double *d_e64, int cb, cudaStream_t stream) {
-    const FieldArgs a = make_args(sys, rs, n_axes, d_axes, d_e64);
-    if (cb == 32) return launch_field_t<32, 8, 4>(a, stream);
-    return launch_field_t<16, 16, 4>(a, stream);
+                 double *d_e64, int cb, int variant, cudaStream_t stream) {
+    FieldArgs a = make_args(sys, rs, n_axes, d_axes, d_e64);
+    sys->split_timed = false;
+    if (rs->r_split >= 1e29 && variant == kPlainVariant) {            // plain FP64 baseline
+        plain_fp64_kernel<<<148 * 16, 256, 0, stream>>>(a);
+        VEXT_CUDA(cudaGetLastError());
+        return 0;
+    }
+    if (rs->r_split >= 1e29) return launch_near(a, cb, 0, stream);   // FP64 oracle
+    // near pairs are at most r_split + 2 (rho + max|offset|) apart
+    double rho = 0;
+    for (const RegionInfo &r : rs->h_info) rho = std::max(rho, r.rho);
+    int near_mode = rs->r_split + 2.0 * (rho + sys->max_offset) + 1e-6 < sys->cutoff ? 2 : 1;
+    if (variant & 256) near_mode = 1;   // keep the cutoff test (study)
+    variant &= ~256;
+    if (!(variant & 16)) {
+        VEXT_TRY(launch_near(a, cb, near_mode, stream));
+        VEXT_CUDA(cudaEventRecord(sys->ev[5], stream));   // near | far split of the timing
+        sys->split_timed = true;
+        return launch_far(a, cb, variant, stream);
+    }
+    variant &= ~16;
+    const size_t n = (size_t)rs->size * rs->size * rs->size * n_axes;
+    VEXT_TRY(ensure_capacity(sys->d_e64b, sys->e64b_cap, n));
+    VEXT_CUDA(cudaEventRecord(sys->fork, stream));
+    VEXT_CUDA(cudaStreamWaitEvent(sys->aux, sys->fork, 0));
+    VEXT_TRY(launch_near(a, cb, near_mode, stream));
+    FieldArgs b = a;
+    b.e64b = sys->d_e64b;
+    VEXT_TRY(launch_far(b, cb, variant, sys->aux));
+    VEXT_CUDA(cudaEventRecord(sys->join, sys->aux));
+    VEXT_CUDA(cudaStreamWaitEvent(stream, sys->join, 0));
+    add_kernel<<<1184, 256, 0, stream>>>(d_e64, sys->d_e64b, (long long)n);
+    VEXT_CUDA(cudaGetLastError());
+    return 0;
 }
 
 // Everything on device pointers and `stream`; region lists are built (with
@@ -436,10 +720,11 @@ static int field_device(System *sys, int size, int n_axes, const double *axes_ho
         return fail(VEXT_ERR_CAPACITY, "size^3 * n_axes must stay below 2^31");
     for (int k = 0; k < 3 * n_axes; ++k)
         if (!std::isfinite(axes_host[k])) return fail(VEXT_ERR_ARGUMENT, "non-finite director");
-    if (o.mode != VEXT_MODE_MIXED && o.mode != VEXT_MODE_FP64)
+    if (o.mode != VEXT_MODE_MIXED && o.mode != VEXT_MODE_FP64 && o.mode != VEXT_MODE_FP64_PLAIN)
         return fail(VEXT_ERR_ARGUMENT, "unknown precision mode %d", o.mode);
     const int cb = o.cb == 32 ? 32 : 16;
-    const double r_split = o.mode == VEXT_MODE_FP64 ? 1e30 : o.r_split;
+    const bool fp64 = o.mode == VEXT_MODE_FP64 || o.mode == VEXT_MODE_FP64_PLAIN;
+    const double r_split = fp64 ? 1e30 : o.r_split;
     RegionSet *rs = nullptr;
     VEXT_TRY(get_field_regions(sys, size, cb, r_split, &rs, stream));
     const size_t n = (size_t)S3 * n_axes;
@@ -453,7 +738,8 @@ static int field_device(System *sys, int size, int n_axes, const double *axes_ho
     VEXT_CUDA(cudaMemsetAsync(sys->d_refine, 0, sizeof(int), stream));
     const FieldArgs a = make_args(sys, rs, n_axes, sys->d_axes, sys->d_e64);
     VEXT_CUDA(cudaEventRecord(sys->ev[0], stream));
-    VEXT_TRY(launch_field(sys, rs, n_axes, sys->d_axes, sys->d_e64, cb, stream));
+    VEXT_TRY(launch_field(sys, rs, n_axes, sys->d_axes, sys->d_e64, cb,
+                          o.mode == VEXT_MODE_FP64_PLAIN ? kPlainVariant : o.variant, stream));
     VEXT_CUDA(cudaEventRecord(sys->ev[1], stream));
     if (o.mode == VEXT_MODE_MIXED && o.band_hi > o.band_lo) {
         flag_kernel<<<592, 256, 0, stream>>>(sys->d_e64, (long long)n, o.band_lo, o.band_hi,
@@ -554,27 +840,32 @@ extern "C" int vext_field_device(vext_system h, int size, int n_axes, const doub
 }
 
 extern "C" int vext_count_pairs(vext_system h, int size, int n_axes, const double *axes,
-                                int64_t *pairs) {
+                                double r_split, int64_t *pairs, int64_t *far_pairs) {
     if (!h || !pairs || !axes || size < 1 || n_axes < 1)
         return fail(VEXT_ERR_ARGUMENT, "bad arguments");
     System *sys = &h->sys;
     std::lock_guard<std::mutex> guard(sys->lock);
     VEXT_CUDA(cudaSetDevice(sys->device));
     cudaStream_t st = sys->stream;
+    vext_options d;
+    vext_default_options(&d);
+    d.r_split = r_split;
+    const Options o = resolve_options(&d);
     RegionSet *rs = nullptr;
-    VEXT_TRY(get_field_regions(sys, size, 16, 1e30, &rs, st));
+    VEXT_TRY(get_field_regions(sys, size, 16, o.r_split, &rs, st));
     VEXT_TRY(ensure_capacity(sys->d_axes, sys->axes_cap, 3 * (size_t)n_axes));
     VEXT_TRY(ensure_capacity(sys->d_flags, sys->flags_cap, 4));
     VEXT_CUDA(cudaMemcpyAsync(sys->d_axes, axes, sizeof(double) * 3 * n_axes,
                               cudaMemcpyHostToDevice, st));
     unsigned long long *total = reinterpret_cast<unsigned long long *>(sys->d_flags);
-    VEXT_CUDA(cudaMemsetAsync(total, 0, sizeof(unsigned long long), st));
+    VEXT_CUDA(cudaMemsetAsync(total, 0, 2 * sizeof(unsigned long long), st));
     const FieldArgs a = make_args(sys, rs, n_axes, sys->d_axes, nullptr);
     count_kernel<<<2368, 256, 0, st>>>(a, total);
     VEXT_CUDA(cudaGetLastError());
-    unsigned long long hcount = 0;
-    VEXT_CUDA(cudaMemcpyAsync(&hcount, total, sizeof hcount, cudaMemcpyDeviceToHost, st));
+    unsigned long long hcount[2] = {0, 0};
+    VEXT_CUDA(cudaMemcpyAsync(hcount, total, sizeof hcount, cudaMemcpyDeviceToHost, st));
     VEXT_CUDA(cudaStreamSynchronize(st));
-    *pairs = (int64_t)hcount;
+    *pairs = (int64_t)hcount[0];
+    if (far_pairs) *far_pairs = (int64_t)hcount[1];
     return 0;
 }

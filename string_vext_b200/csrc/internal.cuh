@@ -89,9 +89,14 @@ struct System {
     void *d_pose_scratch = nullptr;
     size_t pose_scratch_cap = 0;
     cudaStream_t stream = nullptr;   // private stream for host-pointer entries
+    cudaStream_t aux = nullptr;      // second stream: near pairs beside far pairs
+    cudaEvent_t fork = nullptr, join = nullptr;
+    double *d_e64b = nullptr;        // far-pair sums when both kernels run at once
+    size_t e64b_cap = 0;
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     bool timed = false;              // ev[0..2] hold the last field call's kernel/epilogue
     bool list_timed = false;         // ev[3..4] hold the last list build
+    bool split_timed = false;        // ev[5] separates the near and far kernels
     std::mutex lock;
     ~System();
 };
@@ -126,12 +131,13 @@ struct Options {
     double r_split;
     double band_lo, band_hi;
     int cb;
+    int variant;
 };
 Options resolve_options(const vext_options *opt);
 
 // Field kernel launcher (field.cu): computes E64 [O][S^3] for all regions.
 int launch_field(System *sys, const RegionSet *rs, int n_axes, const double *d_axes,
-                 double *d_e64, int cb, cudaStream_t stream);
+                 double *d_e64, int cb, int variant, cudaStream_t stream);
 
 }  // namespace vext
 

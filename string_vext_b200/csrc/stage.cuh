@@ -20,9 +20,13 @@ struct ChunkPlan {
     int n_near, n_total, kn, n_chunks;
 
     __device__ __forceinline__ void init(const RegionInfo &r) {
-        off = r.off;
-        n_near = r.n_near;
-        n_total = r.n_total;
+        init_range(r.off, r.n_near, r.n_total);
+    }
+    // Entries [offset, offset + total) of which the first `near` are near.
+    __device__ __forceinline__ void init_range(long long offset, int near, int total) {
+        off = offset;
+        n_near = near;
+        n_total = total;
         kn = (n_near + kCH - 1) / kCH;
         n_chunks = kn + (n_total - n_near + kCH - 1) / kCH;
     }

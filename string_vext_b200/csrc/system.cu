@@ -50,10 +50,13 @@ Options resolve_options(const vext_options *opt) {
     if (!opt) opt = &d;
     Options o;
     o.mode = opt->mode;
-    o.r_split = opt->r_split > 0 ? opt->r_split : kDefaultRSplit;
+    // Far pairs skip the contact floor, so r_split must exceed every floor
+    // distance 0.1 sigma: it is clamped to at least 1 A.
+    o.r_split = opt->r_split > 0 ? std::max(opt->r_split, 1.0) : kDefaultRSplit;
     o.band_lo = opt->band_lo;
     o.band_hi = opt->band_hi;
     o.cb = opt->centers_per_region;
+    o.variant = opt->variant;
     return o;
 }
 
@@ -424,6 +427,10 @@ System::~System() {
     cudaFree(d_pose_scratch);
     for (auto &e : ev)
         if (e) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    cudaFree(d_e64b);
+    if (aux) cudaStreamDestroy(aux);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -536,6 +543,9 @@ extern "C" int vext_system_create(const vext_system_desc *d, vext_system *out) {
         if (e != cudaSuccess && err == cudaSuccess) err = e;
     };
     chk(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+    chk(cudaStreamCreateWithFlags(&s.aux, cudaStreamNonBlocking));
+    chk(cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming));
+    chk(cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming));
     for (auto &e : s.ev) chk(cudaEventCreate(&e));
     chk(cudaMalloc(&s.d_frac, sizeof(double) * frac.size()));
     chk(cudaMalloc(&s.d_type, sizeof(int) * type.size()));
@@ -565,24 +575,30 @@ extern "C" int vext_system_invalidate(vext_system h) {
     return 0;
 }
 
-extern "C" int vext_last_timings(vext_system h, double *list_ms, double *kernel_ms,
-                                 double *epilogue_ms) {
+extern "C" int vext_last_timings(vext_system h, double *list_ms, double *near_ms,
+                                 double *far_ms, double *epilogue_ms) {
     if (!h) return fail(VEXT_ERR_ARGUMENT, "null system");
     System &s = h->sys;
     std::lock_guard<std::mutex> guard(s.lock);
-    float a = 0, b = 0, c = 0;
+    float a = 0, b = 0, c = 0, d = 0;
     if (s.list_timed) {
         VEXT_CUDA(cudaEventSynchronize(s.ev[4]));
         VEXT_CUDA(cudaEventElapsedTime(&a, s.ev[3], s.ev[4]));
     }
     if (s.timed) {
         VEXT_CUDA(cudaEventSynchronize(s.ev[2]));
-        VEXT_CUDA(cudaEventElapsedTime(&b, s.ev[0], s.ev[1]));
-        VEXT_CUDA(cudaEventElapsedTime(&c, s.ev[1], s.ev[2]));
+        if (s.split_timed) {
+            VEXT_CUDA(cudaEventElapsedTime(&b, s.ev[0], s.ev[5]));
+            VEXT_CUDA(cudaEventElapsedTime(&c, s.ev[5], s.ev[1]));
+        } else {
+            VEXT_CUDA(cudaEventElapsedTime(&b, s.ev[0], s.ev[1]));
+        }
+        VEXT_CUDA(cudaEventElapsedTime(&d, s.ev[1], s.ev[2]));
     }
     if (list_ms) *list_ms = s.list_timed ? a : 0.0;
-    if (kernel_ms) *kernel_ms = s.timed ? b : 0.0;
-    if (epilogue_ms) *epilogue_ms = s.timed ? c : 0.0;
+    if (near_ms) *near_ms = b;
+    if (far_ms) *far_ms = c;
+    if (epilogue_ms) *epilogue_ms = d;
     s.list_timed = false;
     return 0;
 }

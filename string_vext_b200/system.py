@@ -69,19 +69,21 @@ class VextSystem:
         _lib.check(self._lib.vext_system_invalidate(self.handle))
 
     def last_timings(self) -> dict:
-        """Device ms of the last list build, field kernel and epilogue."""
-        vals = [ctypes.c_double() for _ in range(3)]
+        """Device ms of the last list build, near and far pair kernels, epilogue."""
+        vals = [ctypes.c_double() for _ in range(4)]
         _lib.check(self._lib.vext_last_timings(self.handle, *(ctypes.byref(v) for v in vals)))
-        return {"list_ms": vals[0].value, "kernel_ms": vals[1].value,
-                "epilogue_ms": vals[2].value}
+        return {"list_ms": vals[0].value, "near_ms": vals[1].value, "far_ms": vals[2].value,
+                "epilogue_ms": vals[3].value}
 
-    def count_pairs(self, size: int, axes) -> int:
-        """Exact in-cutoff (site, image) pairs of the size^3 x len(axes) field."""
+    def count_pairs(self, size: int, axes, r_split: float = 0.0) -> tuple[int, int]:
+        """Exact in-cutoff (site, image) pairs of the size^3 x len(axes) field:
+        (all pairs, pairs the FP32 far kernel evaluates at this r_split)."""
         axes = _c(axes)
-        out = ctypes.c_int64()
+        total, far = ctypes.c_int64(), ctypes.c_int64()
         _lib.check(self._lib.vext_count_pairs(self.handle, size, len(axes), _lib.ptr(axes),
-                                              ctypes.byref(out)))
-        return out.value
+                                              float(r_split), ctypes.byref(total),
+                                              ctypes.byref(far)))
+        return total.value, far.value
 
     # ------------------------------------------------------------------ field
     def field(self, size: int, axes, mode: int = _lib.VEXT_MODE_MIXED,

@@ -46,8 +46,11 @@ def test_fp64_and_mixed_match_oracle(maker, size, cb):
     ref = oracle.pose_energy(case, centers, axes)
     with VextSystem(case) as system:
         e64 = system.field(size, axes, mode=FP64, energy=True, centers_per_region=cb)["energy"]
+        plain = system.field(size, axes, mode=_lib.VEXT_MODE_FP64_PLAIN, energy=True,
+                             centers_per_region=cb)["energy"]
         mixed = system.field(size, axes, mode=MIXED, energy=True, centers_per_region=cb)
     assert rel(e64, ref).max() < 1e-10
+    assert rel(plain, ref).max() < 1e-10
     assert_mixed_ok(mixed["energy"], ref)
     np.testing.assert_array_equal(mixed["orientation_K"],
                                   mixed["energy"].T.reshape(64, size, size, size).astype(np.float32))
