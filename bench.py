@@ -305,6 +305,9 @@ def run_ours(args, rank, world, local_rank):
         extra["fwd_adjoint"] = {"value": n_pose / (adj_ms * 1e-3), "unit": "poses/s",
                                 "poses": n_pose, "workload": "random poses, same framework",
                                 "flop_per_pair": FLOP_FWD_ADJ}
+        del cart, q, e, gc, gq
+        if not args.no_batch:
+            extra["batch"] = bench_batch(args, size, axes, device, stream)
     if world > 1:
         dist.barrier()
     if rank != 0:
@@ -325,7 +328,7 @@ def run_ours(args, rank, world, local_rank):
             "gpu_launches": args.steps * 7,
             "step_breakdown_ms": {"list_build": list_ms, "near_pairs_fp64": near_ms,
                                   "far_pairs_fp32x2": far_ms, "refine_epilogue": epi_ms},
-            "roofline": {"bound": "fp32", "kernel": "field_far_kernel<16,8,4,4>",
+            "roofline": {"bound": "fp32", "kernel": "field_far_kernel<16,8,4,4> (default variant)",
                          "achieved": achieved_far / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
                          "frac": achieved_far / peak,
                          "peak_source": "measured on this GPU: max(FFMA, FFMA2) FMA rate x 2 "
@@ -341,6 +344,45 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line))
 
 
+def bench_batch(args, size, axes, device, stream):
+    """The batched workload: 50 seeded frameworks x 2 guests = 100 fields of
+    size^3 x 64 in one persistent, graph-captured launch (autotuned)."""
+    import torch
+    from string_vext_b200 import synth
+    from string_vext_b200.system import VextBatch, VextSystem
+    t0 = time.perf_counter()
+    systems = [VextSystem(c) for c in synth.batch_frameworks()]
+    outs = [torch.empty((len(axes), size, size, size), dtype=torch.float32, device=device)
+            for _ in systems]
+    batch = VextBatch(systems, size, axes, outs)
+    setup_s = time.perf_counter() - t0
+    info = batch.info()
+    for _ in range(max(1, args.warmup // 2)):
+        batch.run(stream)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 3
+    a.record(stream)
+    for _ in range(reps):
+        batch.run(stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    batch.check()
+    ms = a.elapsed_time(b) / reps
+    result = {"value": info["poses"] / (ms * 1e-3), "unit": "poses/s", "ms_per_batch": ms,
+              "fields": len(systems), "poses": info["poses"], "work_items": info["work_items"],
+              "list_gb": info["list_bytes"] / 1e9, "setup_s": setup_s,
+              "autotuned": {"cta_shape": ["128x4 dirs", "256x2 dirs"][info["shape"]],
+                            "resident_ctas": info["grid"]},
+              "workload": "50 seeded frameworks x 2 guests, one graph launch"}
+    batch.close()
+    for s_ in systems:
+        s_.close()
+    del outs
+    torch.cuda.empty_cache()
+    return result
+
+
 def main():
     parser = argparse.ArgumentParser(description=__doc__)
     parser.add_argument("--gpus", type=int, default=1)
@@ -352,6 +394,7 @@ def main():
     parser.add_argument("--cpu-seconds", type=float, default=15.0,
                         help="target length of the CPU-baseline sample")
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    parser.add_argument("--no-batch", action="store_true", help="skip the 100-field batch")
     args = parser.parse_args()
     ensure_built()
     world = int(os.environ.get("WORLD_SIZE", "1"))

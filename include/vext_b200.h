@@ -201,6 +201,29 @@ VEXT_API int vext_pose_energy_grad_device(vext_system sys, int n, const double *
                                  void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* Batched fields: many systems (frameworks x guests of uneven sizes and cell
+ * shapes) in one persistent launch over a work queue of (system, region,
+ * 32-director block) items, longest first, captured in a CUDA graph.  The
+ * CTA shape and resident-CTA count are autotuned at creation on a sample of
+ * the queue.  outputs[k] is a DEVICE float32 field [n_axes][S^3] for
+ * systems[k] (mixed precision, with FP64 re-evaluation of the refinement
+ * band).  The systems must outlive the batch and must not be invalidated
+ * while it exists.  No reference counterpart: the reference runs one field
+ * per process (tests/cof/reference_project/graph_vext/cof8948_oldff_vext_exact.py). */
+typedef struct vext_batch_s *vext_batch;
+
+VEXT_API int vext_batch_create(int n_systems, const vext_system *systems, int size, int n_axes,
+                               const double *axes, const vext_options *opt,
+                               float *const *outputs, vext_batch *out);
+/* Replay the captured graph on `stream` (NULL: the batch's own stream). */
+VEXT_API int vext_batch_run(vext_batch batch, void *stream);
+/* Wait for the device and report a timeout or a refinement-list overflow. */
+VEXT_API int vext_batch_status(vext_batch batch);
+VEXT_API int vext_batch_destroy(vext_batch batch);
+VEXT_API int vext_batch_info(vext_batch batch, int64_t *work_items, int64_t *poses,
+                             int64_t *list_bytes, int *shape, int *grid);
+
+/* ------------------------------------------------------------------------ */
 /* Diagnostics. */
 
 /* Non-tensor FP32 FMA throughput of the current device (FLOP/s, FMA = 2),

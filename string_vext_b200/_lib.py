@@ -101,6 +101,18 @@ def load() -> ctypes.CDLL:
     lib.vext_count_pairs.argtypes = [vp, ci, ci, vp, cd, ctypes.POINTER(ctypes.c_int64),
                                      ctypes.POINTER(ctypes.c_int64)]
     lib.vext_count_pairs.restype = ci
+    lib.vext_batch_create.argtypes = [ci, vp, ci, ci, vp, ctypes.POINTER(Options), vp,
+                                      ctypes.POINTER(vp)]
+    lib.vext_batch_create.restype = ci
+    lib.vext_batch_run.argtypes = [vp, vp]
+    lib.vext_batch_run.restype = ci
+    lib.vext_batch_status.argtypes = [vp]
+    lib.vext_batch_status.restype = ci
+    lib.vext_batch_destroy.argtypes = [vp]
+    lib.vext_batch_destroy.restype = ci
+    lib.vext_batch_info.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int64)] * 3 + \
+        [ctypes.POINTER(ci)] * 2
+    lib.vext_batch_info.restype = ci
     lib.vext_measure_pipes.argtypes = [ci] + [ctypes.POINTER(ctypes.c_double)] * 3
     lib.vext_measure_pipes.restype = ci
     lib.vext_measure_fp32_peak.argtypes = [ci, ctypes.POINTER(ctypes.c_double)]

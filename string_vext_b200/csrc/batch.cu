@@ -1,0 +1,478 @@
+// Batched fields: many systems (frameworks x guests of uneven sizes and cell
+// shapes) in ONE persistent launch over a work queue, captured in a CUDA
+// graph and replayed.
+//
+// Work item = (system, region, director block).  Items are sorted by
+// estimated cost (list length, longest first) so the tail of the queue is
+// made of short items; resident CTAs claim items with one atomicAdd each.
+// Each item runs the near (FP64) and the far (packed FP32x2) pair loops of
+// pair.cuh back to back on the same staged-chunk pipeline (the mbarrier
+// phase sequence continues across items) and writes float32 energies
+// straight into the system's [O][S^3] output; poses whose energy falls in the
+// refinement band are appended to a list that batch_refine_kernel
+// recomputes in FP64.
+//
+// Autotuning: the CTA shape (128 threads x 4 directors or 256 threads x 2
+// directors, both covering a 32-director block) and the number of resident
+// CTAs per SM are chosen by timing each candidate on a strided 1/16 sample of
+// the queue at creation; the winner is captured into the graph.  The batch
+// keeps pointers to its systems' region lists: the systems must outlive it
+// and not be invalidated while it exists.
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <numeric>
+#include <vector>
+
+#include "pair.cuh"
+
+namespace vext {
+
+struct BatchSys {
+    Mat3 H;
+    double rc2;
+    float rc2f;
+    double off0, off1;
+    int S, O;
+    const double *axes;
+    const RegionInfo *regs;
+    const float4 *hi, *lo;
+    const float4 *tf;
+    const double *td;
+    int n_types;
+    int near_mode;              // 1: cutoff test on near pairs, 2: none needed
+    int bi, bj, bk, nrj, nrk;   // region grid (pose -> region)
+    float *out;                 // [O][S^3]
+};
+
+struct BatchArgs {
+    const BatchSys *sys;
+    const int4 *items;          // (system, region, director block, -)
+    int n_items;
+    int *counter;
+    int *refine;                // [0] count, then (system, pose) pairs
+    int refine_cap;
+    double band_lo, band_hi;
+    int *status;
+};
+
+template <int CB, int G, int P, int MINB>
+__global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
+    constexpr int NT = CB * G, PP = P / 2;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int s_item;
+    Stager st;
+    st.bar = reinterpret_cast<uint64_t *>(smem);
+    st.hib = reinterpret_cast<float4 *>(smem + 64);
+    st.lob = st.hib + kStages * kCH;
+    double *ed = reinterpret_cast<double *>(st.lob + kStages * kCH);   // [kCH][4]
+    float4 *stf = reinterpret_cast<float4 *>(ed + 4 * kCH);
+    const int tid = threadIdx.x;
+    init_barriers(st);
+    int last_sys = -1;
+    unsigned seq = 0;
+    while (true) {
+        if (tid == 0) s_item = atomicAdd(a.counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= a.n_items) break;
+        const int4 w = a.items[it];
+        const BatchSys &y = a.sys[w.x];
+        double *std4 = reinterpret_cast<double *>(stf + y.n_types);
+        if (w.x != last_sys) {
+            load_types<NT>(stf, std4, y.tf, y.td, y.n_types);
+            last_sys = w.x;
+        }
+        __syncthreads();
+        const RegionInfo r = y.regs[w.y];
+        const int cl = tid % CB, og = tid / CB;
+        const bool cvalid = cl < r.ni * r.nj * r.nk;
+        const int clc = cvalid ? cl : 0;
+        const int gk = r.k0 + clc % r.nk, gj = r.j0 + (clc / r.nk) % r.nj,
+                  gi = r.i0 + clc / (r.nk * r.nj);
+        double cx, cy, cz;
+        frac_to_cart(y.H, (gi + .5) / y.S - r.of[0], (gj + .5) / y.S - r.of[1],
+                     (gk + .5) / y.S - r.of[2], cx, cy, cz);
+        const int obase = w.z * (G * P) + og;
+
+        // ---- near pairs (FP64)
+        double e[P];
+        {
+            double ux[P], uy[P], uz[P], acc[P][2];
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                const int o = min(obase + G * p, y.O - 1);
+                ux[p] = y.axes[3 * o];
+                uy[p] = y.axes[3 * o + 1];
+                uz[p] = y.axes[3 * o + 2];
+                acc[p][0] = acc[p][1] = 0.0;
+            }
+            const NearGeom g = near_geom(cx, cy, cz, y.off0, y.off1, y.rc2);
+            ChunkPlan plan;
+            plan.init_range(r.off, r.n_near, r.n_near);
+            stage_prologue(st, plan, y.hi, y.lo, seq);
+            for (int c = 0; c < plan.n_chunks; ++c) {
+                if (!stage_wait(st, plan, c, seq, a.status)) return;
+                int start, len;
+                bool near;
+                plan.chunk(c, start, len, near);
+                const int s = (seq + c) % kStages;
+                near_convert<NT>(st.hib + s * kCH, st.lob + s * kCH, ed, len);
+                __syncthreads();
+                if (y.near_mode == 2) near_chunk<P, 2>(ed, std4, len, g, ux, uy, uz, acc);
+                else near_chunk<P, 1>(ed, std4, len, g, ux, uy, uz, acc);
+                stage_next(st, plan, y.hi, y.lo, c, seq);
+            }
+            seq += plan.n_chunks;
+#pragma unroll
+            for (int p = 0; p < P; ++p) e[p] = acc[p][0] + acc[p][1];
+        }
+        // ---- far pairs (packed FP32x2)
+        {
+            float2 ux[PP], uy[PP], uz[PP];
+            double acc[P];
+#pragma unroll
+            for (int j = 0; j < PP; ++j) {
+                const int o0 = min(obase + G * (2 * j), y.O - 1);
+                const int o1 = min(obase + G * (2 * j + 1), y.O - 1);
+                ux[j] = make_float2((float)y.axes[3 * o0], (float)y.axes[3 * o1]);
+                uy[j] = make_float2((float)y.axes[3 * o0 + 1], (float)y.axes[3 * o1 + 1]);
+                uz[j] = make_float2((float)y.axes[3 * o0 + 2], (float)y.axes[3 * o1 + 2]);
+                acc[2 * j] = acc[2 * j + 1] = 0.0;
+            }
+            const FarGeom g = far_geom(cx, cy, cz, y.off0, y.off1, y.rc2f);
+            ChunkPlan plan;
+            plan.init_range(r.off + r.n_near, 0, r.n_total - r.n_near);
+            stage_prologue(st, plan, y.hi, y.lo, seq);
+            for (int c = 0; c < plan.n_chunks; ++c) {
+                if (!stage_wait(st, plan, c, seq, a.status)) return;
+                int start, len;
+                bool near;
+                plan.chunk(c, start, len, near);
+                far_chunk<P, true, 16, false, true>(st.hib + ((seq + c) % kStages) * kCH, stf,
+                                                    len, g, ux, uy, uz, acc);
+                stage_next(st, plan, y.hi, y.lo, c, seq);
+            }
+            seq += plan.n_chunks;
+#pragma unroll
+            for (int p = 0; p < P; ++p) e[p] += acc[p];
+        }
+        if (cvalid) {
+            const long long S3 = (long long)y.S * y.S * y.S;
+            const long long cg = ((long long)gi * y.S + gj) * y.S + gk;
+#pragma unroll
+            for (int j = 0; j < PP; ++j)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int o = obase + G * (2 * j + h);
+                    const double v = e[2 * j + h];
+                    if (o < y.O) {
+                        const long long idx = (long long)o * S3 + cg;
+                        y.out[idx] = (float)v;
+                        if (v > a.band_lo && v < a.band_hi) {
+                            const int k = atomicAdd(&a.refine[0], 1);
+                            if (k < a.refine_cap) {
+                                a.refine[1 + 2 * k] = w.x;
+                                a.refine[2 + 2 * k] = (int)idx;
+                            }
+                        }
+                    }
+                }
+        }
+    }
+}
+
+// FP64 re-evaluation of the flagged poses, one warp per pose.
+__global__ void batch_refine_kernel(BatchArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int count = min(a.refine[0], a.refine_cap);
+    for (int q = warp; q < count; q += nwarps) {
+        const BatchSys &y = a.sys[a.refine[1 + 2 * q]];
+        const long long idx = a.refine[2 + 2 * q];
+        const long long S3 = (long long)y.S * y.S * y.S;
+        const int o = (int)(idx / S3);
+        const long long c = idx % S3;
+        const int gi = (int)(c / ((long long)y.S * y.S)), gj = (int)((c / y.S) % y.S),
+                  gk = (int)(c % y.S);
+        const RegionInfo r = y.regs[((gi / y.bi) * y.nrj + gj / y.bj) * y.nrk + gk / y.bk];
+        double cx, cy, cz;
+        frac_to_cart(y.H, (gi + .5) / y.S - r.of[0], (gj + .5) / y.S - r.of[1],
+                     (gk + .5) / y.S - r.of[2], cx, cy, cz);
+        const double ux = y.axes[3 * o], uy = y.axes[3 * o + 1], uz = y.axes[3 * o + 2];
+        double sum = 0.0;
+        for (int s = 0; s < 2; ++s) {
+            const double off = s ? y.off1 : y.off0;
+            const double px = cx + off * ux, py = cy + off * uy, pz = cz + off * uz;
+            for (int k = lane; k < r.n_total; k += 32) {
+                const float4 h = y.hi[r.off + k], l = y.lo[r.off + k];
+                const double dx = px - ((double)h.x + (double)l.x);
+                const double dy = py - ((double)h.y + (double)l.y);
+                const double dz = pz - ((double)h.z + (double)l.z);
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                if (d2 >= y.rc2) continue;
+                const int t = __float_as_int(h.w);
+                const double fl = y.td[4 * t + 3];
+                const double s2 = d2 < fl ? fl : d2;
+                const double i2 = 1.0 / s2;
+                const double i6 = i2 * i2 * i2;
+                sum += y.td[4 * t] * i6 * i6 - y.td[4 * t + 1] * i6 + y.td[4 * t + 2];
+            }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+        if (lane == 0) y.out[idx] = (float)sum;
+    }
+}
+
+// ---------------------------------------------------------------- host side
+
+struct BatchConfig {
+    int shape;   // 0: <16, 8, 4> x 128 threads, 1: <16, 16, 2> x 256 threads (32 directors each)
+    int grid;    // resident CTAs (persistent grid)
+};
+
+}  // namespace vext
+
+using namespace vext;
+
+struct vext_batch_s {
+    std::vector<vext_system> systems;
+    int size = 0, n_axes = 0;
+    Options opt;
+    BatchSys *d_sys = nullptr;
+    int4 *d_items = nullptr, *d_sample = nullptr;
+    int n_items = 0, n_sample = 0;
+    int *d_counter = nullptr, *d_refine = nullptr;
+    int refine_cap = 0;
+    double *d_axes = nullptr;
+    int *d_status = nullptr;
+    int max_types = 0;
+    int64_t poses = 0, list_bytes = 0;
+    BatchConfig config{0, 0};
+    float tune_ms[4] = {0, 0, 0, 0};
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~vext_batch_s() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        cudaFree(d_sys);
+        cudaFree(d_items);
+        cudaFree(d_sample);
+        cudaFree(d_counter);
+        cudaFree(d_refine);
+        cudaFree(d_axes);
+        cudaFree(d_status);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+static size_t batch_smem(int max_types) {
+    return kStageBytes + (size_t)kCH * 4 * sizeof(double) + (size_t)max_types * 48;
+}
+
+static int batch_launch(vext_batch b, const BatchConfig &cfg, const int4 *items, int n_items,
+                        cudaStream_t st) {
+    BatchArgs a;
+    a.sys = b->d_sys;
+    a.items = items;
+    a.n_items = n_items;
+    a.counter = b->d_counter;
+    a.refine = b->d_refine;
+    a.refine_cap = b->refine_cap;
+    a.band_lo = b->opt.band_lo;
+    a.band_hi = b->opt.band_hi;
+    a.status = b->d_status;
+    const size_t smem = batch_smem(b->max_types);
+    VEXT_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(int), st));
+    VEXT_CUDA(cudaMemsetAsync(b->d_refine, 0, sizeof(int), st));
+    if (cfg.shape == 0) {
+        batch_field_kernel<16, 8, 4, 4><<<cfg.grid, 128, smem, st>>>(a);
+    } else {
+        batch_field_kernel<16, 16, 2, 3><<<cfg.grid, 256, smem, st>>>(a);
+    }
+    VEXT_CUDA(cudaGetLastError());
+    if (b->opt.band_hi > b->opt.band_lo) {
+        batch_refine_kernel<<<1184, 256, 0, st>>>(a);
+        VEXT_CUDA(cudaGetLastError());
+    }
+    return 0;
+}
+
+extern "C" int vext_batch_create(int n_systems, const vext_system *systems, int size,
+                                 int n_axes, const double *axes, const vext_options *opt,
+                                 float *const *outputs, vext_batch *out) {
+    if (!out || n_systems < 1 || !systems || !outputs || size < 1 || n_axes < 1 || !axes)
+        return fail(VEXT_ERR_ARGUMENT, "bad batch arguments");
+    *out = nullptr;
+    const long long S3 = (long long)size * size * size;
+    if (S3 * n_axes >= (1LL << 31) - 1)
+        return fail(VEXT_ERR_CAPACITY, "size^3 * n_axes must stay below 2^31");
+    for (int k = 0; k < 3 * n_axes; ++k)
+        if (!std::isfinite(axes[k])) return fail(VEXT_ERR_ARGUMENT, "non-finite director");
+    auto *b = new vext_batch_s();
+    std::unique_ptr<vext_batch_s> guard(b);
+    b->systems.assign(systems, systems + n_systems);
+    b->size = size;
+    b->n_axes = n_axes;
+    b->opt = resolve_options(opt);
+    if (b->opt.mode != VEXT_MODE_MIXED)
+        return fail(VEXT_ERR_ARGUMENT, "batched fields run in the mixed mode only");
+    int dev = 0;
+    VEXT_CUDA(cudaGetDevice(&dev));
+    VEXT_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    VEXT_CUDA(cudaMalloc(&b->d_axes, sizeof(double) * 3 * n_axes));
+    VEXT_CUDA(cudaMemcpy(b->d_axes, axes, sizeof(double) * 3 * n_axes, cudaMemcpyHostToDevice));
+    constexpr int kOB = 32;   // directors per item (both CTA shapes cover 32)
+    std::vector<BatchSys> hs(n_systems);
+    std::vector<std::pair<long long, int4>> items;
+    for (int k = 0; k < n_systems; ++k) {
+        System *sys = &systems[k]->sys;
+        if (sys->device != dev)
+            return fail(VEXT_ERR_ARGUMENT, "system %d lives on another device", k);
+        std::lock_guard<std::mutex> lock(sys->lock);
+        RegionSet *rs = nullptr;
+        VEXT_TRY(get_field_regions(sys, size, 16, b->opt.r_split, &rs, sys->stream));
+        BatchSys &y = hs[k];
+        y.H = sys->H;
+        y.rc2 = sys->cutoff * sys->cutoff;
+        y.rc2f = (float)y.rc2;
+        y.off0 = sys->offsets[0];
+        y.off1 = sys->offsets[1];
+        y.S = size;
+        y.O = n_axes;
+        y.axes = b->d_axes;
+        y.regs = rs->d_info;
+        y.hi = rs->d_hi;
+        y.lo = rs->d_lo;
+        y.tf = sys->d_tf;
+        y.td = sys->d_td;
+        y.n_types = sys->n_types;
+        double rho = 0;
+        for (const RegionInfo &r : rs->h_info) rho = std::max(rho, r.rho);
+        y.near_mode = rs->r_split + 2.0 * (rho + sys->max_offset) + 1e-6 < sys->cutoff ? 2 : 1;
+        y.bi = rs->bi;
+        y.bj = rs->bj;
+        y.bk = rs->bk;
+        y.nrj = rs->n_rj;
+        y.nrk = rs->n_rk;
+        y.out = outputs[k];
+        b->max_types = std::max(b->max_types, sys->n_types);
+        b->poses += S3 * n_axes;
+        b->list_bytes += rs->n_entries * 32;
+        for (int ri = 0; ri < rs->n_regions; ++ri)
+            for (int ob = 0; ob < (n_axes + kOB - 1) / kOB; ++ob)
+                items.push_back({(long long)rs->h_info[ri].n_total, make_int4(k, ri, ob, 0)});
+    }
+    // longest items first
+    std::stable_sort(items.begin(), items.end(),
+                     [](const auto &x, const auto &y) { return x.first > y.first; });
+    std::vector<int4> hitems(items.size());
+    for (size_t i = 0; i < items.size(); ++i) hitems[i] = items[i].second;
+    b->n_items = (int)hitems.size();
+    std::vector<int4> sample;
+    for (size_t i = 0; i < hitems.size(); i += 16) sample.push_back(hitems[i]);
+    b->n_sample = (int)sample.size();
+    VEXT_CUDA(cudaMalloc(&b->d_sys, sizeof(BatchSys) * n_systems));
+    VEXT_CUDA(cudaMemcpy(b->d_sys, hs.data(), sizeof(BatchSys) * n_systems, cudaMemcpyHostToDevice));
+    VEXT_CUDA(cudaMalloc(&b->d_items, sizeof(int4) * hitems.size()));
+    VEXT_CUDA(cudaMemcpy(b->d_items, hitems.data(), sizeof(int4) * hitems.size(),
+                         cudaMemcpyHostToDevice));
+    VEXT_CUDA(cudaMalloc(&b->d_sample, sizeof(int4) * sample.size()));
+    VEXT_CUDA(cudaMemcpy(b->d_sample, sample.data(), sizeof(int4) * sample.size(),
+                         cudaMemcpyHostToDevice));
+    VEXT_CUDA(cudaMalloc(&b->d_counter, sizeof(int)));
+    b->refine_cap = (int)std::min<long long>(b->poses / 16 + 1024, 8 << 20);
+    VEXT_CUDA(cudaMalloc(&b->d_refine, sizeof(int) * (1 + 2 * (size_t)b->refine_cap)));
+    VEXT_CUDA(cudaMalloc(&b->d_status, sizeof(int)));
+    VEXT_CUDA(cudaMemset(b->d_status, 0, sizeof(int)));
+    // ---- autotune: CTA shape x resident CTAs per SM, on the sampled queue
+    const size_t smem = batch_smem(b->max_types);
+    VEXT_CUDA(cudaFuncSetAttribute(batch_field_kernel<16, 8, 4, 4>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    VEXT_CUDA(cudaFuncSetAttribute(batch_field_kernel<16, 16, 2, 3>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int sms = 0, occ0 = 0, occ1 = 0;
+    VEXT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    VEXT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, batch_field_kernel<16, 8, 4, 4>,
+                                                            128, smem));
+    VEXT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, batch_field_kernel<16, 16, 2, 3>,
+                                                            256, smem));
+    if (occ0 < 1 || occ1 < 1) return fail(VEXT_ERR_CAPACITY, "batch kernel does not fit an SM");
+    const BatchConfig cands[4] = {{0, sms * occ0}, {0, sms * std::max(1, occ0 / 2)},
+                                  {1, sms * occ1}, {1, sms * std::max(1, occ1 / 2)}};
+    cudaEvent_t e0, e1;
+    VEXT_CUDA(cudaEventCreate(&e0));
+    VEXT_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    for (int c = 0; c < 4; ++c) {
+        VEXT_TRY(batch_launch(b, cands[c], b->d_sample, b->n_sample, b->stream));   // warm-up
+        VEXT_CUDA(cudaEventRecord(e0, b->stream));
+        VEXT_TRY(batch_launch(b, cands[c], b->d_sample, b->n_sample, b->stream));
+        VEXT_CUDA(cudaEventRecord(e1, b->stream));
+        VEXT_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        VEXT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        b->tune_ms[c] = ms;
+        if (ms < best) {
+            best = ms;
+            b->config = cands[c];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int status = 0;
+    VEXT_CUDA(cudaMemcpy(&status, b->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status) return fail(VEXT_ERR_TIMEOUT, "a device wait gave up during batch tuning");
+    // ---- capture the whole batch into a graph
+    VEXT_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = batch_launch(b, b->config, b->d_items, b->n_items, b->stream);
+    cudaGraph_t g = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(b->stream, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    VEXT_CUDA(end);
+    b->graph = g;
+    VEXT_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    *out = guard.release();
+    return 0;
+}
+
+extern "C" int vext_batch_run(vext_batch b, void *stream) {
+    if (!b) return fail(VEXT_ERR_ARGUMENT, "null batch");
+    VEXT_CUDA(cudaGraphLaunch(b->exec, stream ? (cudaStream_t)stream : b->stream));
+    return 0;
+}
+
+extern "C" int vext_batch_status(vext_batch b) {
+    if (!b) return fail(VEXT_ERR_ARGUMENT, "null batch");
+    int h[2] = {0, 0};
+    VEXT_CUDA(cudaDeviceSynchronize());
+    VEXT_CUDA(cudaMemcpy(&h[0], b->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    VEXT_CUDA(cudaMemcpy(&h[1], b->d_refine, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h[0]) return fail(VEXT_ERR_TIMEOUT, "a device wait gave up (status %d)", h[0]);
+    if (h[1] > b->refine_cap)
+        return fail(VEXT_ERR_CAPACITY, "%d poses in the refinement band; %d refined", h[1],
+                    b->refine_cap);
+    return 0;
+}
+
+extern "C" int vext_batch_destroy(vext_batch b) {
+    delete b;
+    return 0;
+}
+
+extern "C" int vext_batch_info(vext_batch b, int64_t *work_items, int64_t *poses,
+                               int64_t *list_bytes, int *shape, int *grid) {
+    if (!b) return fail(VEXT_ERR_ARGUMENT, "null batch");
+    if (work_items) *work_items = b->n_items;
+    if (poses) *poses = b->poses;
+    if (list_bytes) *list_bytes = b->list_bytes;
+    if (shape) *shape = b->config.shape;
+    if (grid) *grid = b->config.grid;
+    return 0;
+}

@@ -1,27 +1,23 @@
 // Vext field kernels: every (grid center, director) pose of a size^3 grid.
 //
 // One CTA = one region (a block of CB grid centers) x one block of G*P
-// directors; thread (cl, og) owns center cl and directors og + G p
-// (p < P), i.e. 2P guest sites held in registers in FP64 and FP32,
-// relative to the region origin.  The region's list is streamed through
-// shared memory in kCH-entry chunks by bulk copies (stage.cuh); every staged
-// entry is used by all 2P sites of all threads.
+// directors; thread (cl, og) owns center cl and directors og + G p (p < P).
+// The region's list streams through shared memory in kCH-entry chunks by
+// bulk copies (stage.cuh); every staged entry is used by all 2P sites of all
+// threads.  The pair loops live in pair.cuh.
 //
-// Precision: near chunks (entries within r_split + max|offset| + rho of the
-// origin) are evaluated in FP64 from the exact hi + lo positions; far chunks
-// in FP32 from hi, with an IEEE-rounded reciprocal refined by one Newton
-// step, accumulated in FP32 over 16 entries and then flushed into the FP64
-// per-site sum.  Poses whose energy falls in the refinement band (where the
-// 1e-6 relative criterion is tighter than the FP32 error) are recomputed in
-// FP64 by refine_kernel.  With r_split = infinity every entry is near: that
-// is the FP64 oracle kernel.
-//
-// Pair term (native/vext/kernel.cpp:26-36 and neighbor.py:21-28):
-//   d2 < rc^2:  s2 = max(d2, floor2), i6 = 1/s2^3, e = c12 i6^2 - c6 i6 + shift.
+// Precision: near entries (within r_split + max|offset| + rho of the origin)
+// go through field_near_kernel in FP64 from the exact hi + lo positions; far
+// entries through field_far_kernel in packed FP32x2 from hi, accumulated in
+// FP32 over 16 entries and flushed into FP64.  Poses whose energy falls in
+// the refinement band (where the 1e-6 relative criterion is tighter than the
+// FP32 error) are recomputed in FP64 by refine_kernel.  With r_split =
+// infinity every entry is near: field_near_kernel<..., 0> is then the FP64
+// oracle kernel; plain_fp64_kernel is the straightforward FP64 baseline.
 #include <algorithm>
 #include <cmath>
 
-#include "stage.cuh"
+#include "pair.cuh"
 
 namespace vext {
 
@@ -54,70 +50,8 @@ __device__ __forceinline__ void center_of(const FieldArgs &a, const RegionInfo &
     gk = r.k0 + lk;
 }
 
-// Shared set-up of both pair kernels: barriers, type tables, first copies.
-template <int NT>
-__device__ __forceinline__ void stage_begin(Stager &st, const ChunkPlan &plan, const FieldArgs &a,
-                                            float4 *stf, double *std4) {
-    const int tid = threadIdx.x;
-    for (int t = tid; t < a.n_types; t += NT) {
-        stf[t] = a.tf[t];
-        if (std4)
-#pragma unroll
-            for (int k = 0; k < 4; ++k) std4[4 * t + k] = a.td[4 * t + k];
-    }
-    if (tid == 0) {
-        for (int s = 0; s < kStages; ++s) mbar_init(&st.bar[s], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-    if (tid == 0)
-        for (int c = 0; c < min(kStages, plan.n_chunks); ++c) st.issue(plan, a.hi, a.lo, c, c);
-}
-
-// Wait for chunk c; on a failed wait drain the copies in flight and report
-// false (the whole CTA then returns).
-__device__ __forceinline__ bool stage_wait(Stager &st, const ChunkPlan &plan, int c, int *status) {
-    const bool ok = mbar_wait_bounded(&st.bar[c % kStages], (c / kStages) & 1, status);
-    if (__syncthreads_and(ok)) return true;
-    if (threadIdx.x == 0)
-        for (int cc = c; cc < min(c + kStages, plan.n_chunks); ++cc)
-            mbar_drain(&st.bar[cc % kStages], (cc / kStages) & 1);
-    return false;
-}
-
-__device__ __forceinline__ void stage_next(Stager &st, const ChunkPlan &plan, const FieldArgs &a,
-                                           int c) {
-    __syncthreads();
-    if (threadIdx.x == 0 && c + kStages < plan.n_chunks)
-        st.issue(plan, a.hi, a.lo, c + kStages, c + kStages);
-}
-
-
-__device__ __forceinline__ float set_lt(float a, float b) {
-    float r;
-    asm("set.lt.f32.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
-    return r;
-}
-
-// FP64 reciprocal: hardware seed refined by two Newton-Raphson steps
-// r' = r + r (1 - s r).  Each step squares the relative error; one step
-// leaves a measurable one-sided (under-estimating) bias, two do not.
-__device__ __forceinline__ double rcp64_nr(double s) {
-    double r;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(s));
-    r = fma(r, fma(-s, r, 1.0), r);
-    return fma(r, fma(-s, r, 1.0), r);
-}
-
-// Near pairs in FP64: E[pose] = sum over the region's near entries (all
-// entries for the FP64 oracle region set).
-//   MODE 0 (the FP64 oracle kernel): direct d = site - x per site, IEEE
-//          reciprocal, cutoff test.
-//   MODE 1/2 (mixed precision): every thread's poses share one grid center
-//          c, so with d0 = x - c, t = d0 . u:  q_s = |d0|^2 + o_s^2 - 2 o_s t
-//          (|d0|^2 once per entry, 1 FMA per site after t); Newton-refined
-//          reciprocal.  MODE 2 drops the cutoff test: near pairs are never
-//          farther apart than r_split + 2 rho_site < rc (checked on the host).
+// Near pairs in FP64 over every region's near entries (all entries for the
+// FP64 oracle region set); MODE as in near_chunk (pair.cuh).  Writes e64.
 template <int CB, int G, int P, int MODE>
 __global__ void __launch_bounds__(CB *G, 1) field_near_kernel(FieldArgs a) {
     constexpr int NT = CB * G;
@@ -134,7 +68,10 @@ __global__ void __launch_bounds__(CB *G, 1) field_near_kernel(FieldArgs a) {
     const RegionInfo r = a.regs[blockIdx.x];
     ChunkPlan plan;
     plan.init_range(r.off, r.n_near, r.n_near);
-    stage_begin<NT>(st, plan, a, stf, std4);
+    load_types<NT>(stf, std4, a.tf, a.td, a.n_types);
+    init_barriers(st);
+    __syncthreads();
+    stage_prologue(st, plan, a.hi, a.lo, 0);
 
     const int cl = tid % CB, og = tid / CB;
     const bool cvalid = cl < r.ni * r.nj * r.nk;
@@ -143,6 +80,7 @@ __global__ void __launch_bounds__(CB *G, 1) field_near_kernel(FieldArgs a) {
     double cx, cy, cz;
     frac_to_cart(a.H, (gi + .5) / a.S - r.of[0], (gj + .5) / a.S - r.of[1],
                  (gk + .5) / a.S - r.of[2], cx, cy, cz);
+    const NearGeom g = near_geom(cx, cy, cz, a.off0, a.off1, a.rc2);
     const int obase = blockIdx.y * (G * P) + og;
     double ux[P], uy[P], uz[P];
     double acc[P][2];
@@ -154,66 +92,16 @@ __global__ void __launch_bounds__(CB *G, 1) field_near_kernel(FieldArgs a) {
         uz[p] = a.axes[3 * o + 2];
         acc[p][0] = acc[p][1] = 0.0;
     }
-    const double m0 = -2.0 * a.off0, m1 = -2.0 * a.off1;
-    const double oo0 = a.off0 * a.off0, oo1 = a.off1 * a.off1;
     for (int c = 0; c < plan.n_chunks; ++c) {
-        if (!stage_wait(st, plan, c, a.status)) return;
+        if (!stage_wait(st, plan, c, 0, a.status)) return;
         int start, len;
         bool near;
         plan.chunk(c, start, len, near);
         const int s = c % kStages;
-        const float4 *hb = st.hib + s * kCH, *lb = st.lob + s * kCH;
-        for (int e = tid; e < len; e += NT) {
-            const float4 h = hb[e], l = lb[e];
-            ed[4 * e + 0] = (double)h.x + (double)l.x;
-            ed[4 * e + 1] = (double)h.y + (double)l.y;
-            ed[4 * e + 2] = (double)h.z + (double)l.z;
-            ed[4 * e + 3] = (double)__float_as_int(h.w);
-        }
+        near_convert<NT>(st.hib + s * kCH, st.lob + s * kCH, ed, len);
         __syncthreads();
-        const double2 *ed2 = reinterpret_cast<const double2 *>(ed);
-        const double2 *td2 = reinterpret_cast<const double2 *>(std4);
-#pragma unroll 1
-        for (int e = 0; e < len; ++e) {
-            const double2 xy = ed2[2 * e], zt = ed2[2 * e + 1];
-            const int t = (int)zt.y;
-            const double2 cc = td2[2 * t], sh = td2[2 * t + 1];   // (c12, c6), (shift, floor2)
-            if (MODE == 0) {
-#pragma unroll
-                for (int p = 0; p < P; ++p)
-#pragma unroll
-                    for (int q = 0; q < 2; ++q) {
-                        const double off = q ? a.off1 : a.off0;
-                        const double dx = cx + off * ux[p] - xy.x, dy = cy + off * uy[p] - xy.y,
-                                     dz = cz + off * uz[p] - zt.x;
-                        const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
-                        const double s2 = fmax(d2, sh.y);
-                        const double i2 = __drcp_rn(s2);
-                        const double i6 = i2 * i2 * i2;
-                        const double en = fma(i6, fma(cc.x, i6, -cc.y), sh.x);
-                        acc[p][q] += d2 < a.rc2 ? en : 0.0;
-                    }
-            } else {
-                const double dx = xy.x - cx, dy = xy.y - cy, dz = zt.x - cz;
-                const double dd = fma(dx, dx, fma(dy, dy, dz * dz));
-                const double k0 = dd + oo0, k1 = dd + oo1;
-#pragma unroll
-                for (int p = 0; p < P; ++p) {
-                    const double tt = fma(dx, ux[p], fma(dy, uy[p], dz * uz[p]));
-#pragma unroll
-                    for (int q = 0; q < 2; ++q) {
-                        const double d2 = fma(q ? m1 : m0, tt, q ? k1 : k0);
-                        const double s2 = fmax(d2, sh.y);
-                        const double i2 = rcp64_nr(s2);
-                        const double i6 = i2 * i2 * i2;
-                        const double en = fma(i6, fma(cc.x, i6, -cc.y), sh.x);
-                        if (MODE == 1) acc[p][q] += d2 < a.rc2 ? en : 0.0;
-                        else acc[p][q] += en;
-                    }
-                }
-            }
-        }
-        stage_next(st, plan, a, c);
+        near_chunk<P, MODE>(ed, std4, len, g, ux, uy, uz, acc);
+        stage_next(st, plan, a.hi, a.lo, c, 0);
     }
     if (cvalid) {
         const size_t S3 = (size_t)a.S * a.S * a.S;
@@ -226,22 +114,12 @@ __global__ void __launch_bounds__(CB *G, 1) field_near_kernel(FieldArgs a) {
     }
 }
 
-// Far pairs in packed FP32x2.  A thread owns one grid center c and P
-// directors; lanes .x/.y of a float2 hold two directors (p, p + 1).  Per
-// staged entry x (image relative to the region origin):
-//   d0 = x - c, D = |d0|^2 (scalar, once per entry; with CLO corrected by
-//        -2 d0 . c_lo, c_lo the FP32 rounding residual of the center),
-//   t = d0 . u  (packed over two directors),
-//   q_s = (D + o_s^2) - 2 o_s t  = |x - (c + o_s u)|^2  for site s;
-//   one hardware reciprocal per two pairs: nr = 1/(-q.x q.y),
-//   n = (q.y nr, q.x nr) = -1/q, refined by one Newton step n' = n + n(1 + q n);
-//   n3 = n'^3 = -1/q^3, e = n3 (c12 n3 + c6) + shift = c12/q^6 - c6/q^3 + shift;
-//   a 1/0 mask (q < rc^2) multiplies e into the FP32 partial sums, flushed
-//   into FP64 every 16 entries.
-// Far entries are >= r_split from every site, so no pair reaches the contact
-// floor.  The far sums are added into e64 (written by the near kernel) or
-// stored into e64b.
-template <int CB, int G, int P, int MINB, bool NEWTON = true, int FLUSH = 16, bool CLO = false>
+// Far pairs in packed FP32x2 over every region's far entries (far_chunk,
+// pair.cuh).  A thread owns one grid center and P directors (lanes of a
+// float2 = two directors).  The far sums are added into e64 (written by the
+// near kernel) or stored into e64b.
+template <int CB, int G, int P, int MINB, bool NEWTON = true, int FLUSH = 16, bool CLO = false,
+          bool RCP3 = false>
 __global__ void __launch_bounds__(CB *G, MINB) field_far_kernel(FieldArgs a) {
     static_assert(P % 2 == 0, "directors are packed in pairs");
     constexpr int NT = CB * G, PP = P / 2;
@@ -256,7 +134,10 @@ __global__ void __launch_bounds__(CB *G, MINB) field_far_kernel(FieldArgs a) {
     const RegionInfo r = a.regs[blockIdx.x];
     ChunkPlan plan;
     plan.init_range(r.off + r.n_near, 0, r.n_total - r.n_near);
-    stage_begin<NT>(st, plan, a, stf, nullptr);
+    load_types<NT>(stf, nullptr, a.tf, a.td, a.n_types);
+    init_barriers(st);
+    __syncthreads();
+    stage_prologue(st, plan, a.hi, a.lo, 0);
 
     const int cl = tid % CB, og = tid / CB;
     const bool cvalid = cl < r.ni * r.nj * r.nk;
@@ -265,11 +146,7 @@ __global__ void __launch_bounds__(CB *G, MINB) field_far_kernel(FieldArgs a) {
     double cxd, cyd, czd;
     frac_to_cart(a.H, (gi + .5) / a.S - r.of[0], (gj + .5) / a.S - r.of[1],
                  (gk + .5) / a.S - r.of[2], cxd, cyd, czd);
-    const float cx = (float)cxd, cy = (float)cyd, cz = (float)czd;
-    // FP32 residual of the center (used by the CLO variant: it removes the
-    // coherent displacement grad(E) . dc that rounding c gives every far pair
-    // of this thread, to first order in |x - c|^2).
-    const float cxl = (float)(cxd - cx), cyl = (float)(cyd - cy), czl = (float)(czd - cz);
+    const FarGeom g = far_geom(cxd, cyd, czd, a.off0, a.off1, a.rc2f);
     const int obase = blockIdx.y * (G * P) + og;
     float2 ux[PP], uy[PP], uz[PP];
     double acc[P];
@@ -281,59 +158,14 @@ __global__ void __launch_bounds__(CB *G, MINB) field_far_kernel(FieldArgs a) {
         uz[j] = make_float2((float)a.axes[3 * o0 + 2], (float)a.axes[3 * o1 + 2]);
         acc[2 * j] = acc[2 * j + 1] = 0.0;
     }
-    const float2 m0 = make_float2(-2.f * (float)a.off0, -2.f * (float)a.off0);
-    const float2 m1 = make_float2(-2.f * (float)a.off1, -2.f * (float)a.off1);
-    const float oo0 = (float)(a.off0 * a.off0), oo1 = (float)(a.off1 * a.off1);
-    const float2 one2 = make_float2(1.f, 1.f);
-    const float rc2f = a.rc2f;
     for (int c = 0; c < plan.n_chunks; ++c) {
-        if (!stage_wait(st, plan, c, a.status)) return;
+        if (!stage_wait(st, plan, c, 0, a.status)) return;
         int start, len;
         bool near;
         plan.chunk(c, start, len, near);
-        const float4 *hb = st.hib + (c % kStages) * kCH;
-#pragma unroll 1
-        for (int e0 = 0; e0 < len; e0 += FLUSH) {
-            float2 fa[PP];
-#pragma unroll
-            for (int j = 0; j < PP; ++j) fa[j] = make_float2(0.f, 0.f);
-            const int e1 = min(e0 + FLUSH, len);
-#pragma unroll 2
-            for (int e = e0; e < e1; ++e) {
-                const float4 h = hb[e];
-                const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, floor2)
-                const float dx = h.x - cx, dy = h.y - cy, dz = h.z - cz;
-                float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                if (CLO) dd = fmaf(-2.f, fmaf(dx, cxl, fmaf(dy, cyl, dz * czl)), dd);
-                const float2 k0 = make_float2(dd + oo0, dd + oo0), k1 = make_float2(dd + oo1, dd + oo1);
-                const float2 dx2 = make_float2(dx, dx), dy2 = make_float2(dy, dy),
-                             dz2 = make_float2(dz, dz);
-                const float2 c12 = make_float2(tp.x, tp.x), c6 = make_float2(tp.y, tp.y),
-                             sh = make_float2(tp.z, tp.z);
-#pragma unroll
-                for (int j = 0; j < PP; ++j) {
-                    const float2 t = __ffma2_rn(dx2, ux[j], __ffma2_rn(dy2, uy[j], __fmul2_rn(dz2, uz[j])));
-#pragma unroll
-                    for (int q = 0; q < 2; ++q) {
-                        const float2 d2 = __ffma2_rn(q ? m1 : m0, t, q ? k1 : k0);
-                        float nr;
-                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(nr) : "f"(-d2.x * d2.y));
-                        float2 n = make_float2(d2.y * nr, d2.x * nr);
-                        if (NEWTON) n = __ffma2_rn(n, __ffma2_rn(d2, n, one2), n);
-                        const float2 n3 = __fmul2_rn(__fmul2_rn(n, n), n);
-                        const float2 en = __ffma2_rn(n3, __ffma2_rn(c12, n3, c6), sh);
-                        const float2 m = make_float2(set_lt(d2.x, rc2f), set_lt(d2.y, rc2f));
-                        fa[j] = __ffma2_rn(en, m, fa[j]);
-                    }
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < PP; ++j) {
-                acc[2 * j] += (double)fa[j].x;
-                acc[2 * j + 1] += (double)fa[j].y;
-            }
-        }
-        stage_next(st, plan, a, c);
+        far_chunk<P, NEWTON, FLUSH, CLO, RCP3>(st.hib + (c % kStages) * kCH, stf, len, g, ux, uy,
+                                               uz, acc);
+        stage_next(st, plan, a.hi, a.lo, c, 0);
     }
     if (cvalid) {
         const size_t S3 = (size_t)a.S * a.S * a.S;
@@ -606,9 +438,10 @@ static int launch_near(const FieldArgs &a, int cb, int mode, cudaStream_t stream
 }
 
 // Far-kernel variants (threads = CB x G, directors per CTA = G x P):
-//   0/5 (default): <16, 8, 4>, 4 CTAs/SM of 128      1: <16, 16, 4>, 2 CTAs/SM
-//   2: <16, 32, 2>, 1 CTA of 512/SM    3: <16, 16, 2>, 3 CTAs/SM
-//   4: <16, 16, 4>, 3 CTAs/SM
+//   0 (default): <16, 8, 4>, 4 CTAs/SM of 128, one reciprocal of q^3 per lane
+//   5: the same with one reciprocal per two lanes (1/(qx qy)) and cubing
+//   1: <16, 16, 4>, 2 CTAs/SM    2: <16, 32, 2>, 1 CTA of 512/SM
+//   3: <16, 16, 2>, 3 CTAs/SM    4: <16, 16, 4>, 3 CTAs/SM
 // cb = 32 uses <32, 8, 4>.
 static int launch_far(const FieldArgs &a, int cb, int variant, cudaStream_t stream) {
     const size_t smem = far_smem(a.n_types);
@@ -616,6 +449,8 @@ static int launch_far(const FieldArgs &a, int cb, int variant, cudaStream_t stre
     if (cb == 32) return launch_t(field_far_kernel<32, 8, 4, 2>, grid_for(32), 256, smem, a, stream);
     if (variant & 32)   // without the Newton step (accuracy study)
         return launch_t(field_far_kernel<16, 16, 4, 2, false>, grid_for(64), 256, smem, a, stream);
+    if (variant == 10)  // ... without the Newton step
+        return launch_t(field_far_kernel<16, 8, 4, 4, false, 16, false, true>, grid_for(32), 128, smem, a, stream);
     if (variant == 8)   // with the first-order centre-residual correction
         return launch_t(field_far_kernel<16, 8, 4, 4, true, 16, true>, grid_for(32), 128, smem, a, stream);
     if (variant & 64)   // FP32 partial sums flushed every 8 entries
@@ -627,7 +462,10 @@ static int launch_far(const FieldArgs &a, int cb, int variant, cudaStream_t stre
     case 3: return launch_t(field_far_kernel<16, 16, 2, 3>, grid_for(32), 256, smem, a, stream);
     case 4: return launch_t(field_far_kernel<16, 16, 4, 3>, grid_for(64), 256, smem, a, stream);
     case 1: return launch_t(field_far_kernel<16, 16, 4, 2>, grid_for(64), 256, smem, a, stream);
-    default: return launch_t(field_far_kernel<16, 8, 4, 4>, grid_for(32), 128, smem, a, stream);
+    case 5: return launch_t(field_far_kernel<16, 8, 4, 4>, grid_for(32), 128, smem, a, stream);
+    default:
+        return launch_t(field_far_kernel<16, 8, 4, 4, true, 16, false, true>, grid_for(32), 128,
+                        smem, a, stream);
     }
 }
 

@@ -1,0 +1,275 @@
+// Pair loops shared by the per-field kernels (field.cu) and the persistent
+// batched kernel (batch.cu): the staging protocol of one region's list and
+// the per-chunk FP64 (near) and packed FP32x2 (far) pair sums.
+//
+// Pair term (native/vext/kernel.cpp:26-36 and neighbor.py:21-28):
+//   d2 < rc^2:  s2 = max(d2, floor2), i6 = 1/s2^3, e = c12 i6^2 - c6 i6 + shift.
+#pragma once
+
+#include "stage.cuh"
+
+namespace vext {
+
+__device__ __forceinline__ float set_lt(float a, float b) {
+    float r;
+    asm("set.lt.f32.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
+
+// FP64 reciprocal: hardware seed refined by two Newton-Raphson steps
+// r' = r + r (1 - s r).  Each step squares the relative error; one step
+// leaves a measurable one-sided (under-estimating) bias, two do not.
+__device__ __forceinline__ double rcp64_nr(double s) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(s));
+    r = fma(r, fma(-s, r, 1.0), r);
+    return fma(r, fma(-s, r, 1.0), r);
+}
+
+// ------------------------------------------------------------ staging
+
+template <int NT>
+__device__ __forceinline__ void load_types(float4 *stf, double *std4, const float4 *tf,
+                                           const double *td, int n_types) {
+    for (int t = threadIdx.x; t < n_types; t += NT) {
+        stf[t] = tf[t];
+        if (std4)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) std4[4 * t + k] = td[4 * t + k];
+    }
+}
+
+__device__ __forceinline__ void init_barriers(Stager &st) {
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) mbar_init(&st.bar[s], 1);
+        fence_mbar_init();
+    }
+}
+
+// Chunk c of `plan` is the seq0 + c-th chunk this CTA stages: stage
+// (seq0 + c) % kStages, phase parity ((seq0 + c) / kStages) & 1.
+__device__ __forceinline__ void stage_prologue(Stager &st, const ChunkPlan &plan,
+                                               const float4 *hi, const float4 *lo,
+                                               unsigned seq0) {
+    if (threadIdx.x == 0)
+        for (int c = 0; c < min(kStages, plan.n_chunks); ++c) st.issue(plan, hi, lo, c, seq0 + c);
+}
+
+// Wait for chunk c; on a failed wait drain the copies in flight and report
+// false (the whole CTA must then return).
+__device__ __forceinline__ bool stage_wait(Stager &st, const ChunkPlan &plan, int c,
+                                           unsigned seq0, int *status) {
+    const unsigned q = seq0 + c;
+    const bool ok = mbar_wait_bounded(&st.bar[q % kStages], (q / kStages) & 1, status);
+    if (__syncthreads_and(ok)) return true;
+    if (threadIdx.x == 0)
+        for (int cc = c; cc < min(c + kStages, plan.n_chunks); ++cc)
+            mbar_drain(&st.bar[(seq0 + cc) % kStages], ((seq0 + cc) / kStages) & 1);
+    return false;
+}
+
+// All threads are done with chunk c: reuse its stage for chunk c + kStages.
+__device__ __forceinline__ void stage_next(Stager &st, const ChunkPlan &plan, const float4 *hi,
+                                           const float4 *lo, int c, unsigned seq0) {
+    __syncthreads();
+    if (threadIdx.x == 0 && c + kStages < plan.n_chunks)
+        st.issue(plan, hi, lo, c + kStages, seq0 + c + kStages);
+}
+
+// Staged near chunk (hi + lo) -> FP64 (x, y, z, type) in shared memory.
+template <int NT>
+__device__ __forceinline__ void near_convert(const float4 *hb, const float4 *lb, double *ed,
+                                             int len) {
+    for (int e = threadIdx.x; e < len; e += NT) {
+        const float4 h = hb[e], l = lb[e];
+        ed[4 * e + 0] = (double)h.x + (double)l.x;
+        ed[4 * e + 1] = (double)h.y + (double)l.y;
+        ed[4 * e + 2] = (double)h.z + (double)l.z;
+        ed[4 * e + 3] = (double)__float_as_int(h.w);
+    }
+}
+
+// ------------------------------------------------------------ near (FP64)
+
+struct NearGeom {
+    double cx, cy, cz;        // grid center relative to the region origin
+    double off0, off1;        // site offsets
+    double m0, m1, oo0, oo1;  // -2 o_s and o_s^2
+    double rc2;
+};
+
+__device__ __forceinline__ NearGeom near_geom(double cx, double cy, double cz, double off0,
+                                              double off1, double rc2) {
+    NearGeom g;
+    g.cx = cx;
+    g.cy = cy;
+    g.cz = cz;
+    g.off0 = off0;
+    g.off1 = off1;
+    g.m0 = -2.0 * off0;
+    g.m1 = -2.0 * off1;
+    g.oo0 = off0 * off0;
+    g.oo1 = off1 * off1;
+    g.rc2 = rc2;
+    return g;
+}
+
+// Sum one converted near chunk into acc[p][site] for the thread's P directors.
+//   MODE 0 (FP64 oracle): direct d = site - x per site, IEEE reciprocal,
+//          cutoff test.
+//   MODE 1/2 (mixed): the thread's poses share one grid center c, so with
+//          d0 = x - c, t = d0 . u:  q_s = |d0|^2 + o_s^2 - 2 o_s t (|d0|^2
+//          once per entry, 1 FMA per site after t); Newton-refined
+//          reciprocal.  MODE 2 drops the cutoff test (near pairs are never
+//          farther apart than r_split + 2 rho_site < rc, checked on the host).
+template <int P, int MODE>
+__device__ __forceinline__ void near_chunk(const double *ed, const double *std4, int len,
+                                           const NearGeom &g, const double (&ux)[P],
+                                           const double (&uy)[P], const double (&uz)[P],
+                                           double (&acc)[P][2]) {
+    const double2 *ed2 = reinterpret_cast<const double2 *>(ed);
+    const double2 *td2 = reinterpret_cast<const double2 *>(std4);
+#pragma unroll 1
+    for (int e = 0; e < len; ++e) {
+        const double2 xy = ed2[2 * e], zt = ed2[2 * e + 1];
+        const int t = (int)zt.y;
+        const double2 cc = td2[2 * t], sh = td2[2 * t + 1];   // (c12, c6), (shift, floor2)
+        if (MODE == 0) {
+#pragma unroll
+            for (int p = 0; p < P; ++p)
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const double off = q ? g.off1 : g.off0;
+                    const double dx = g.cx + off * ux[p] - xy.x, dy = g.cy + off * uy[p] - xy.y,
+                                 dz = g.cz + off * uz[p] - zt.x;
+                    const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
+                    const double s2 = fmax(d2, sh.y);
+                    const double i2 = __drcp_rn(s2);
+                    const double i6 = i2 * i2 * i2;
+                    const double en = fma(i6, fma(cc.x, i6, -cc.y), sh.x);
+                    acc[p][q] += d2 < g.rc2 ? en : 0.0;
+                }
+        } else {
+            const double dx = xy.x - g.cx, dy = xy.y - g.cy, dz = zt.x - g.cz;
+            const double dd = fma(dx, dx, fma(dy, dy, dz * dz));
+            const double k0 = dd + g.oo0, k1 = dd + g.oo1;
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                const double tt = fma(dx, ux[p], fma(dy, uy[p], dz * uz[p]));
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const double d2 = fma(q ? g.m1 : g.m0, tt, q ? k1 : k0);
+                    const double s2 = fmax(d2, sh.y);
+                    const double i2 = rcp64_nr(s2);
+                    const double i6 = i2 * i2 * i2;
+                    const double en = fma(i6, fma(cc.x, i6, -cc.y), sh.x);
+                    if (MODE == 1) acc[p][q] += d2 < g.rc2 ? en : 0.0;
+                    else acc[p][q] += en;
+                }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------ far (FP32x2)
+
+struct FarGeom {
+    float cx, cy, cz;          // grid center (FP32) relative to the region origin
+    float cxl, cyl, czl;       // its FP32 rounding residual (CLO variant)
+    float2 m0, m1;             // -2 o_s, broadcast
+    float oo0, oo1;            // o_s^2
+    float rc2f;
+};
+
+__device__ __forceinline__ FarGeom far_geom(double cxd, double cyd, double czd, double off0,
+                                            double off1, float rc2f) {
+    FarGeom g;
+    g.cx = (float)cxd;
+    g.cy = (float)cyd;
+    g.cz = (float)czd;
+    g.cxl = (float)(cxd - g.cx);
+    g.cyl = (float)(cyd - g.cy);
+    g.czl = (float)(czd - g.cz);
+    g.m0 = make_float2(-2.f * (float)off0, -2.f * (float)off0);
+    g.m1 = make_float2(-2.f * (float)off1, -2.f * (float)off1);
+    g.oo0 = (float)(off0 * off0);
+    g.oo1 = (float)(off1 * off1);
+    g.rc2f = rc2f;
+    return g;
+}
+
+// Sum one staged far chunk (hi only) into acc[p] (both sites) for the
+// thread's P directors, packed two per float2 (lanes = directors p, p + 1).
+// Per entry x:  d0 = x - c, D = |d0|^2 (scalar, once; with CLO corrected by
+// -2 d0 . c_lo), t = d0 . u (packed), q_s = (D + o_s^2) - 2 o_s t.
+//   RCP3: n3 = hardware reciprocal of -q^3 per lane, refined (NEWTON) by
+//         n3' = n3 + n3 (1 + q^3 n3);
+//   else: one reciprocal per two lanes nr = 1/(-q.x q.y), n = (q.y nr, q.x nr)
+//         = -1/q, refined likewise, n3 = n^3.
+// Either way n3 = -1/q^3 and e = n3 (c12 n3 + c6) + shift = c12/q^6 -
+// c6/q^3 + shift; a 1/0 mask (q < rc^2) multiplies e into FP32 partial sums
+// flushed into FP64 every FLUSH entries.  Far entries are >= r_split from
+// every site, so no pair reaches the contact floor (no max()).
+template <int P, bool NEWTON, int FLUSH, bool CLO, bool RCP3>
+__device__ __forceinline__ void far_chunk(const float4 *hb, const float4 *stf, int len,
+                                          const FarGeom &g, const float2 (&ux)[P / 2],
+                                          const float2 (&uy)[P / 2], const float2 (&uz)[P / 2],
+                                          double (&acc)[P]) {
+    constexpr int PP = P / 2;
+    const float2 one2 = make_float2(1.f, 1.f);
+#pragma unroll 1
+    for (int e0 = 0; e0 < len; e0 += FLUSH) {
+        float2 fa[PP];
+#pragma unroll
+        for (int j = 0; j < PP; ++j) fa[j] = make_float2(0.f, 0.f);
+        const int e1 = min(e0 + FLUSH, len);
+#pragma unroll 2
+        for (int e = e0; e < e1; ++e) {
+            const float4 h = hb[e];
+            const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, floor2)
+            const float dx = h.x - g.cx, dy = h.y - g.cy, dz = h.z - g.cz;
+            float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if (CLO) dd = fmaf(-2.f, fmaf(dx, g.cxl, fmaf(dy, g.cyl, dz * g.czl)), dd);
+            const float2 k0 = make_float2(dd + g.oo0, dd + g.oo0),
+                         k1 = make_float2(dd + g.oo1, dd + g.oo1);
+            const float2 dx2 = make_float2(dx, dx), dy2 = make_float2(dy, dy),
+                         dz2 = make_float2(dz, dz);
+            const float2 c12 = make_float2(tp.x, tp.x), c6 = make_float2(tp.y, tp.y),
+                         sh = make_float2(tp.z, tp.z);
+#pragma unroll
+            for (int j = 0; j < PP; ++j) {
+                const float2 t =
+                    __ffma2_rn(dx2, ux[j], __ffma2_rn(dy2, uy[j], __fmul2_rn(dz2, uz[j])));
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const float2 d2 = __ffma2_rn(q ? g.m1 : g.m0, t, q ? k1 : k0);
+                    float2 n3;
+                    if (RCP3) {
+                        const float2 d6 = __fmul2_rn(__fmul2_rn(d2, d2), d2);
+                        float r0, r1;
+                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(-d6.x));
+                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r1) : "f"(-d6.y));
+                        n3 = make_float2(r0, r1);
+                        if (NEWTON) n3 = __ffma2_rn(n3, __ffma2_rn(d6, n3, one2), n3);
+                    } else {
+                        float nr;
+                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(nr) : "f"(-d2.x * d2.y));
+                        float2 n = make_float2(d2.y * nr, d2.x * nr);
+                        if (NEWTON) n = __ffma2_rn(n, __ffma2_rn(d2, n, one2), n);
+                        n3 = __fmul2_rn(__fmul2_rn(n, n), n);
+                    }
+                    const float2 en = __ffma2_rn(n3, __ffma2_rn(c12, n3, c6), sh);
+                    const float2 m = make_float2(set_lt(d2.x, g.rc2f), set_lt(d2.y, g.rc2f));
+                    fa[j] = __ffma2_rn(en, m, fa[j]);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < PP; ++j) {
+            acc[2 * j] += (double)fa[j].x;
+            acc[2 * j + 1] += (double)fa[j].y;
+        }
+    }
+}
+
+}  // namespace vext

@@ -154,3 +154,49 @@ class VextSystem:
             self.handle, int(centers.shape[0]), _lib.ptr(centers), _lib.ptr(quats),
             ctypes.byref(opt), _lib.ptr(energy), _lib.ptr(grad_center), _lib.ptr(grad_quat),
             _lib.ptr(grad_director), handle))
+
+
+class VextBatch:
+    """Many systems' fields in one persistent, graph-captured launch
+    (``vext_batch_create``).  ``outputs`` are CUDA float32 tensors
+    [n_axes, S, S, S], one per system; ``run()`` replays the graph."""
+
+    def __init__(self, systems, size: int, axes, outputs, **opts):
+        self._lib = _lib.load()
+        self.systems = list(systems)           # kept alive: the batch points into them
+        self.outputs = list(outputs)
+        self.axes = _c(axes)
+        handles = (ctypes.c_void_p * len(self.systems))(*[s.handle.value for s in self.systems])
+        outs = (ctypes.c_void_p * len(self.outputs))(*[o.data_ptr() for o in self.outputs])
+        opt = _lib.options(_lib.VEXT_MODE_MIXED, **opts)
+        handle = ctypes.c_void_p()
+        _lib.check(self._lib.vext_batch_create(len(self.systems), handles, size, len(self.axes),
+                                               _lib.ptr(self.axes), ctypes.byref(opt), outs,
+                                               ctypes.byref(handle)))
+        self.handle = handle
+
+    def run(self, stream=None) -> None:
+        h = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        _lib.check(self._lib.vext_batch_run(self.handle, h))
+
+    def check(self) -> None:
+        _lib.check(self._lib.vext_batch_status(self.handle))
+
+    def info(self) -> dict:
+        a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        d, e = ctypes.c_int(), ctypes.c_int()
+        _lib.check(self._lib.vext_batch_info(self.handle, ctypes.byref(a), ctypes.byref(b),
+                                             ctypes.byref(c), ctypes.byref(d), ctypes.byref(e)))
+        return {"work_items": a.value, "poses": b.value, "list_bytes": c.value,
+                "shape": d.value, "grid": e.value}
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self._lib.vext_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
