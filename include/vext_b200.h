@@ -201,6 +201,42 @@ VEXT_API int vext_pose_energy_grad_device(vext_system sys, int n, const double *
                                  void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* GPU String path update.  Replaces the iteration loop of the reference
+ * String solver (native/string/source_code/RC_main.cu:1914-2420 with the
+ * kernels of global.h:1281-2244): per-block normalised steepest-descent step,
+ * end fixing along the transport axis, equal-arc-length reparametrisation of
+ * the positions, energy check of the new angles, angle smoothing, movement-
+ * based convergence test every check_every iterations -- the same rules and
+ * constants -- with the finite-difference forces replaced by h x the analytic
+ * gradient.  path is HOST [n][6] (fractional a, b, c; Euler alpha, beta,
+ * gamma in radians, R = Rz(gamma) Ry(beta) Rx(alpha)), updated in place;
+ * energy (may be NULL) receives the final energies [n]. */
+typedef struct {
+    int direction;             /* transport axis 1 = a, 2 = b, 3 = c            */
+    double delta_frac;         /* step / difference size in fractional units    */
+    double delta_angle_rad;    /* angular step (reference: 1 degree)            */
+    double smooth;             /* angle smoothing coefficient (1e-4)            */
+    double rounding;           /* truncation quantum (1e-15)                    */
+    double conv_trans_percent; /* convergence thresholds (30 %)                 */
+    double conv_rot_percent;
+    int max_iterations;        /* Running_steps                                 */
+    int check_every;           /* convergence test period (200)                 */
+} vext_string_params;
+
+typedef struct {
+    int iterations;            /* iterations run (the reference's i_time)       */
+    int converged;             /* both blocks below threshold at a test         */
+    int converged_translation, converged_rotation;
+    double movement_translation, movement_rotation;   /* last iteration        */
+    double threshold_translation, threshold_rotation;
+} vext_string_result;
+
+VEXT_API void vext_string_default_params(vext_string_params *params);
+VEXT_API int vext_string_run(vext_system sys, int n_images, double *path, double *energy,
+                             const vext_string_params *params, const vext_options *opt,
+                             vext_string_result *result);
+
+/* ------------------------------------------------------------------------ */
 /* Batched fields: many systems (frameworks x guests of uneven sizes and cell
  * shapes) in one persistent launch over a work queue of (system, region,
  * 32-director block) items, longest first, captured in a CUDA graph.  The

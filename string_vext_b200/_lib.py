@@ -50,6 +50,26 @@ class FieldStats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class StringParams(ctypes.Structure):
+    _fields_ = [("direction", ctypes.c_int), ("delta_frac", ctypes.c_double),
+                ("delta_angle_rad", ctypes.c_double), ("smooth", ctypes.c_double),
+                ("rounding", ctypes.c_double), ("conv_trans_percent", ctypes.c_double),
+                ("conv_rot_percent", ctypes.c_double), ("max_iterations", ctypes.c_int),
+                ("check_every", ctypes.c_int)]
+
+
+class StringResult(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("converged", ctypes.c_int),
+                ("converged_translation", ctypes.c_int), ("converged_rotation", ctypes.c_int),
+                ("movement_translation", ctypes.c_double),
+                ("movement_rotation", ctypes.c_double),
+                ("threshold_translation", ctypes.c_double),
+                ("threshold_rotation", ctypes.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class VextError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(f"vext_b200 status {code} ({STATUS.get(code, '?')}): {message}")
@@ -113,6 +133,11 @@ def load() -> ctypes.CDLL:
     lib.vext_batch_info.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int64)] * 3 + \
         [ctypes.POINTER(ci)] * 2
     lib.vext_batch_info.restype = ci
+    lib.vext_string_default_params.argtypes = [ctypes.POINTER(StringParams)]
+    lib.vext_string_default_params.restype = None
+    lib.vext_string_run.argtypes = [vp, ci, vp, vp, ctypes.POINTER(StringParams),
+                                    ctypes.POINTER(Options), ctypes.POINTER(StringResult)]
+    lib.vext_string_run.restype = ci
     lib.vext_measure_pipes.argtypes = [ci] + [ctypes.POINTER(ctypes.c_double)] * 3
     lib.vext_measure_pipes.restype = ci
     lib.vext_measure_fp32_peak.argtypes = [ci, ctypes.POINTER(ctypes.c_double)]

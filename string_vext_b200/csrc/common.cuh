@@ -35,7 +35,7 @@ int fail(int code, const char *fmt, ...);
     } while (0)
 
 // Device status word values (written by kernels, read by the host).
-enum : int { DEV_OK = 0, DEV_TIMEOUT = 1, DEV_BAD_LIST = 2 };
+enum : int { DEV_OK = 0, DEV_TIMEOUT = 1, DEV_BAD_LIST = 2, DEV_BAD_INPUT = 3 };
 
 // Upper bound on spin iterations of one mbarrier wait (each try_wait also
 // suspends in hardware for a while, so this is about a second of wall time).

@@ -88,6 +88,8 @@ struct System {
     // scratch of the pose path
     void *d_pose_scratch = nullptr;
     size_t pose_scratch_cap = 0;
+    double *d_pose_io = nullptr;     // host-pointer entry staging
+    size_t pose_io_cap = 0;
     cudaStream_t stream = nullptr;   // private stream for host-pointer entries
     cudaStream_t aux = nullptr;      // second stream: near pairs beside far pairs
     cudaEvent_t fork = nullptr, join = nullptr;
@@ -126,6 +128,7 @@ int ensure_capacity(T *&ptr, size_t &cap, size_t need) {
 
 int check_status(System *sys, cudaStream_t stream);  // reads and clears the status word
 
+
 struct Options {
     int mode;
     double r_split;
@@ -134,6 +137,12 @@ struct Options {
     int variant;
 };
 Options resolve_options(const vext_options *opt);
+
+// Pose pipeline (pose.cu): enqueue without host synchronisation, then check.
+int pose_enqueue(System *sys, int n, const double *centers, const double *quats,
+                 const Options &o, double *energy, double *gc, double *gq, double *gu,
+                 cudaStream_t st);
+int pose_status(System *sys, cudaStream_t st);
 
 // Field kernel launcher (field.cu): computes E64 [O][S^3] for all regions.
 int launch_field(System *sys, const RegionSet *rs, int n_axes, const double *d_axes,

@@ -49,7 +49,7 @@ struct PoseArgs {
     int *status;
 };
 
-enum : int { DEV_BAD_INPUT = 3 };
+
 
 __global__ void pose_prep_kernel(PoseArgs a) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -404,9 +404,13 @@ static size_t pose_scratch_bytes(int n, int n_bins, int max_items, bool host_io)
     return b + 256;
 }
 
-static int pose_run(System *sys, int n, const double *centers, const double *quats,
-                    const Options &o, double *energy, double *gc, double *gq, double *gu,
-                    cudaStream_t st, bool host_io) {
+// Enqueue the whole pose pipeline on `st` (device pointers, no host
+// synchronisation once the bin lists exist; safe inside stream capture after
+// a first call has built the lists and the scratch).  Energies go to `energy`
+// (a scratch buffer when NULL).
+int pose_enqueue(System *sys, int n, const double *centers, const double *quats,
+                 const Options &o, double *energy, double *gc, double *gq, double *gu,
+                 cudaStream_t st) {
     if (n < 0) return fail(VEXT_ERR_ARGUMENT, "negative pose count");
     if (n == 0) return 0;
     if (!centers || !quats) return fail(VEXT_ERR_ARGUMENT, "centers and quaternions required");
@@ -417,7 +421,7 @@ static int pose_run(System *sys, int n, const double *centers, const double *qua
     VEXT_TRY(get_bin_regions(sys, r_split, &rs, st));
     const int n_bins = rs->n_regions;
     const int max_items = n_bins + (n + kPoseThreads - 1) / kPoseThreads;
-    const size_t bytes = pose_scratch_bytes(n, n_bins, max_items, host_io);
+    const size_t bytes = pose_scratch_bytes(n, n_bins, max_items, false);
     VEXT_TRY(ensure_capacity(*reinterpret_cast<char **>(&sys->d_pose_scratch),
                              sys->pose_scratch_cap, bytes));
     Bump bump{reinterpret_cast<char *>(sys->d_pose_scratch)};
@@ -455,26 +459,12 @@ static int pose_run(System *sys, int n, const double *centers, const double *qua
     a.band_hi = o.band_hi;
     a.status = sys->d_status;
     double *e_tmp = bump.take<double>(n);
-    const double *in_c = centers, *in_q = quats;
-    double *out_gc = gc, *out_gq = gq, *out_gu = gu;
-    if (host_io) {
-        double *dc = bump.take<double>(3 * (size_t)n), *dq = bump.take<double>(4 * (size_t)n);
-        VEXT_CUDA(cudaMemcpyAsync(dc, centers, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
-        VEXT_CUDA(cudaMemcpyAsync(dq, quats, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, st));
-        in_c = dc;
-        in_q = dq;
-        double *dgc = bump.take<double>(3 * (size_t)n), *dgq = bump.take<double>(4 * (size_t)n),
-               *dgu = bump.take<double>(3 * (size_t)n);
-        out_gc = gc ? dgc : nullptr;
-        out_gq = gq ? dgq : nullptr;
-        out_gu = gu ? dgu : nullptr;
-    }
-    a.centers = in_c;
-    a.quats = in_q;
-    a.energy = (energy && !host_io) ? energy : e_tmp;
-    a.gc = out_gc;
-    a.gq = out_gq;
-    a.gu = out_gu;
+    a.centers = centers;
+    a.quats = quats;
+    a.energy = energy ? energy : e_tmp;
+    a.gc = gc;
+    a.gq = gq;
+    a.gu = gu;
     VEXT_CUDA(cudaMemsetAsync(a.counts, 0, sizeof(int) * n_bins, st));
     VEXT_CUDA(cudaMemsetAsync(a.cursor, 0, sizeof(int) * n_bins, st));
     VEXT_CUDA(cudaMemsetAsync(d_refine, 0, sizeof(int), st));
@@ -494,16 +484,32 @@ static int pose_run(System *sys, int n, const double *centers, const double *qua
         pose_refine_kernel<<<std::min(1184, (n + 7) / 8), 256, 0, st>>>(a);
         VEXT_CUDA(cudaGetLastError());
     }
-    if (host_io) {
-        if (energy)
-            VEXT_CUDA(cudaMemcpyAsync(energy, a.energy, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
-        if (gc)
-            VEXT_CUDA(cudaMemcpyAsync(gc, out_gc, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st));
-        if (gq)
-            VEXT_CUDA(cudaMemcpyAsync(gq, out_gq, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, st));
-        if (gu)
-            VEXT_CUDA(cudaMemcpyAsync(gu, out_gu, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st));
-    }
+    return 0;
+}
+
+// Host-pointer wrapper: copies in, pose_enqueue, copies out, status check.
+static int pose_run_host(System *sys, int n, const double *centers, const double *quats,
+                         const Options &o, double *energy, double *gc, double *gq, double *gu,
+                         cudaStream_t st) {
+    if (n < 0) return fail(VEXT_ERR_ARGUMENT, "negative pose count");
+    if (n == 0) return 0;
+    if (!centers || !quats) return fail(VEXT_ERR_ARGUMENT, "centers and quaternions required");
+    const size_t per = sizeof(double) * (size_t)n;
+    VEXT_TRY(ensure_capacity(sys->d_pose_io, sys->pose_io_cap, 18 * (size_t)n));
+    double *dc = sys->d_pose_io, *dq = dc + 3 * (size_t)n, *de = dq + 4 * (size_t)n,
+           *dgc = de + n, *dgq = dgc + 3 * (size_t)n, *dgu = dgq + 4 * (size_t)n;
+    VEXT_CUDA(cudaMemcpyAsync(dc, centers, 3 * per, cudaMemcpyHostToDevice, st));
+    VEXT_CUDA(cudaMemcpyAsync(dq, quats, 4 * per, cudaMemcpyHostToDevice, st));
+    VEXT_TRY(pose_enqueue(sys, n, dc, dq, o, de, gc ? dgc : nullptr, gq ? dgq : nullptr,
+                          gu ? dgu : nullptr, st));
+    if (energy) VEXT_CUDA(cudaMemcpyAsync(energy, de, per, cudaMemcpyDeviceToHost, st));
+    if (gc) VEXT_CUDA(cudaMemcpyAsync(gc, dgc, 3 * per, cudaMemcpyDeviceToHost, st));
+    if (gq) VEXT_CUDA(cudaMemcpyAsync(gq, dgq, 4 * per, cudaMemcpyDeviceToHost, st));
+    if (gu) VEXT_CUDA(cudaMemcpyAsync(gu, dgu, 3 * per, cudaMemcpyDeviceToHost, st));
+    return pose_status(sys, st);
+}
+
+int pose_status(System *sys, cudaStream_t st) {
     int status = 0;
     VEXT_CUDA(cudaMemcpyAsync(&status, sys->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
     VEXT_CUDA(cudaStreamSynchronize(st));
@@ -529,8 +535,8 @@ extern "C" int vext_pose_energy_grad(vext_system h, int n, const double *centers
     System *sys = &h->sys;
     std::lock_guard<std::mutex> guard(sys->lock);
     VEXT_CUDA(cudaSetDevice(sys->device));
-    return pose_run(sys, n, centers, quats, resolve_options(opt), energy, grad_center, grad_quat,
-                    grad_director, sys->stream, true);
+    return pose_run_host(sys, n, centers, quats, resolve_options(opt), energy, grad_center,
+                         grad_quat, grad_director, sys->stream);
 }
 
 extern "C" int vext_pose_energy_grad_device(vext_system h, int n, const double *centers,
@@ -542,6 +548,8 @@ extern "C" int vext_pose_energy_grad_device(vext_system h, int n, const double *
     System *sys = &h->sys;
     std::lock_guard<std::mutex> guard(sys->lock);
     VEXT_CUDA(cudaSetDevice(sys->device));
-    return pose_run(sys, n, centers, quats, resolve_options(opt), energy, grad_center, grad_quat,
-                    grad_director, (cudaStream_t)stream, false);
+    cudaStream_t st = (cudaStream_t)stream;
+    VEXT_TRY(pose_enqueue(sys, n, centers, quats, resolve_options(opt), energy, grad_center,
+                          grad_quat, grad_director, st));
+    return pose_status(sys, st);
 }

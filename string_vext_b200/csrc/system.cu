@@ -425,6 +425,7 @@ System::~System() {
     cudaFree(d_e64T);
     cudaFree(d_flags);
     cudaFree(d_pose_scratch);
+    cudaFree(d_pose_io);
     for (auto &e : ev)
         if (e) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
