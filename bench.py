@@ -38,6 +38,9 @@ sys.path.insert(0, str(ROOT))
 FLOP_FWD = 16          # algorithmic FLOP per in-cutoff (site, image) pair, forward
 FLOP_FWD_ADJ = 28      # forward + adjoint
 METRIC = "Vext pose evals/s at <=1e-4 K vs FP64, fwd+adjoint evals/s; % FP32 peak"
+# dram__bytes_read.sum + dram__bytes_write.sum of one field_far_kernel launch on
+# full_field, from an ncu capture (--set full) of `bench.py --profile field`.
+FAR_DRAM_BYTES_FULL_FIELD = 741_898_752 + 101_475_584
 CPU_CENTERS_PER_CORE_S = 900.0   # reference driver throughput estimate used to size the sample
 
 
@@ -334,7 +337,9 @@ def run_ours(args, rank, world, local_rank):
                          "peak_source": "measured on this GPU: max(FFMA, FFMA2) FMA rate x 2 "
                                         "(vext_measure_pipes); MEASURED_PEAKS.json has no FP32 figure",
                          "algorithmic": f"{far_pairs} far in-cutoff pairs x {FLOP_FWD} FLOP per field",
-                         "traffic": None,
+                         "traffic": (FAR_DRAM_BYTES_FULL_FIELD
+                                     if args.workload == "full_field" else None),
+                         "traffic_unit": "bytes per launch (ncu dram__bytes_read+write)",
                          "both_pair_kernels": {"achieved": achieved_pairs / 1e12,
                                                "frac": achieved_pairs / peak,
                                                "algorithmic": f"{pairs} in-cutoff pairs x {FLOP_FWD} FLOP"},
@@ -383,6 +388,33 @@ def bench_batch(args, size, axes, device, stream):
     return result
 
 
+def run_profile_case(kind):
+    """Short, fixed cases for ncu (no timing is reported from them)."""
+    import torch
+    from string_vext_b200 import synth
+    from string_vext_b200.orientation import normalized_directors, regular_pose_grid
+    from string_vext_b200.system import VextSystem
+    case = synth.full_field()
+    with VextSystem(case) as system:
+        if kind == "field":
+            _, axes = regular_pose_grid(60, 64)
+            axes = normalized_directors(axes)
+            for _ in range(2):
+                system.field(60, axes, orientation=False)
+        else:
+            n = 1 << 20
+            rng = np.random.default_rng(9)
+            cart = torch.tensor(rng.random((n, 3)) @ case["cell"], device="cuda")
+            q = torch.tensor(rng.normal(size=(n, 4)), device="cuda")
+            e = torch.empty(n, dtype=torch.float64, device="cuda")
+            gc = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+            gq = torch.empty((n, 4), dtype=torch.float64, device="cuda")
+            for _ in range(2):
+                system.pose_energy_grad_device(cart, q, e, gc, gq)
+            torch.cuda.synchronize()
+    print(f"profile case {kind} done")
+
+
 def main():
     parser = argparse.ArgumentParser(description=__doc__)
     parser.add_argument("--gpus", type=int, default=1)
@@ -395,8 +427,15 @@ def main():
                         help="target length of the CPU-baseline sample")
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     parser.add_argument("--no-batch", action="store_true", help="skip the 100-field batch")
+    parser.add_argument("--profile", choices=("field", "pose"),
+                        help="run one short case for an ncu capture and exit: 'field' = two "
+                             "mixed full_field fields, 'pose' = two 2^20-pose forward+adjoint "
+                             "batches of the same framework")
     args = parser.parse_args()
     ensure_built()
+    if args.profile:
+        run_profile_case(args.profile)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
