@@ -177,6 +177,35 @@ VEXT_API int vext_field_device(vext_system sys, int size, int n_axes, const doub
                       const vext_options *opt, float *orientation_K, double *energy_f64,
                       float *marginal_K, float *site_K, float *grid, void *stream);
 
+/* Forward + adjoint over the field poses: energy and gradient of every
+ * (grid center, director) pose of the size^3 x n_axes field (same centers,
+ * directors and [n_axes][S^3] pose order as vext_field).  DEVICE outputs on
+ * `stream` (cudaStream_t as void*):
+ *   energy        float32 [n_axes][S^3]     E, K
+ *   gradient      float32 [n_axes][S^3][6]  dE/d(center) (K/A, Cartesian),
+ *                                          then dE/du projected on the plane
+ *                                          normal to u (K per unit director)
+ *   energy_f64    double [n_axes][S^3]     the energies before float32 rounding
+ *                                          (NULL to skip)
+ *   gradient_f64  double [n_axes][S^3][6]  FP64 modes only (NULL to skip)
+ * VEXT_MODE_MIXED runs the persistent batched kernel (FP64 near pairs, packed
+ * FP32 far pairs with FP64-flushed partial sums, FP64 energy refinement band)
+ * on a one-system batch that is built, autotuned and graph-captured on the
+ * first call and replayed while (size, directors, options, outputs) stay the
+ * same; VEXT_MODE_FP64 and VEXT_MODE_FP64_PLAIN run the plain one-thread-per-
+ * pose FP64 kernel (IEEE division), the FP64 reference of the adjoint.  No
+ * reference counterpart: the reference has no field gradient; its String
+ * solver differentiates by forward differences
+ * (native/string/source_code/global.h:1141-1325). */
+VEXT_API int vext_field_adjoint_device(vext_system sys, int size, int n_axes,
+                                       const double *axes_host, const vext_options *opt,
+                                       float *energy, float *gradient, double *energy_f64,
+                                       double *gradient_f64, void *stream);
+/* Same with HOST float32 outputs (staged on the device, copied back before
+ * the call returns). */
+VEXT_API int vext_field_adjoint(vext_system sys, int size, int n_axes, const double *axes,
+                                const vext_options *opt, float *energy, float *gradient);
+
 /* ------------------------------------------------------------------------ */
 /* Pose energies and the analytic adjoint for arbitrary poses.  A pose is a
  * Cartesian center (A) and a quaternion q = (w, x, y, z), used normalised;
@@ -251,6 +280,13 @@ typedef struct vext_batch_s *vext_batch;
 VEXT_API int vext_batch_create(int n_systems, const vext_system *systems, int size, int n_axes,
                                const double *axes, const vext_options *opt,
                                float *const *outputs, vext_batch *out);
+/* Forward + adjoint batch: energies[k] as outputs above, gradients[k] a
+ * DEVICE float32 [n_axes][S^3][6] array (dE/d(center), tangent dE/du; layout
+ * of vext_field_adjoint_device).  Same queue, autotuning and graph. */
+VEXT_API int vext_batch_create_adjoint(int n_systems, const vext_system *systems, int size,
+                                       int n_axes, const double *axes, const vext_options *opt,
+                                       float *const *energies, float *const *gradients,
+                                       vext_batch *out);
 /* Replay the captured graph on `stream` (NULL: the batch's own stream). */
 VEXT_API int vext_batch_run(vext_batch batch, void *stream);
 /* Wait for the device and report a timeout or a refinement-list overflow. */

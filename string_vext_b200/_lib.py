@@ -124,6 +124,14 @@ def load() -> ctypes.CDLL:
     lib.vext_batch_create.argtypes = [ci, vp, ci, ci, vp, ctypes.POINTER(Options), vp,
                                       ctypes.POINTER(vp)]
     lib.vext_batch_create.restype = ci
+    lib.vext_batch_create_adjoint.argtypes = [ci, vp, ci, ci, vp, ctypes.POINTER(Options), vp,
+                                              vp, ctypes.POINTER(vp)]
+    lib.vext_batch_create_adjoint.restype = ci
+    lib.vext_field_adjoint_device.argtypes = [vp, ci, ci, vp, ctypes.POINTER(Options), vp, vp,
+                                              vp, vp, vp]
+    lib.vext_field_adjoint_device.restype = ci
+    lib.vext_field_adjoint.argtypes = [vp, ci, ci, vp, ctypes.POINTER(Options), vp, vp]
+    lib.vext_field_adjoint.restype = ci
     lib.vext_batch_run.argtypes = [vp, vp]
     lib.vext_batch_run.restype = ci
     lib.vext_batch_status.argtypes = [vp]

@@ -43,6 +43,8 @@ struct BatchSys {
     int near_mode;              // 1: cutoff test on near pairs, 2: none needed
     int bi, bj, bk, nrj, nrk;   // region grid (pose -> region)
     float *out;                 // [O][S^3]
+    float *grad;                // [O][S^3][6] (forward + adjoint batches), else null
+    double *out64;              // FP64 copy of the energies [O][S^3], or null
 };
 
 struct BatchArgs {
@@ -56,7 +58,79 @@ struct BatchArgs {
     int *status;
 };
 
-template <int CB, int G, int P, int MINB>
+// Forward + adjoint item: the same staged pipeline with the AdjAcc pair loops
+// (pair.cuh); writes the energy and [dE/dc, tangent dE/du] of every pose.
+template <int CB, int G, int P>
+__device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSys &y,
+                                               const RegionInfo &r, Stager &st, double *ed,
+                                               const float4 *stf, const double *std4,
+                                               unsigned &seq, double cx, double cy, double cz,
+                                               int obase, double (&e)[P], double (&gr)[P][6]) {
+    constexpr int NT = CB * G, PP = P / 2;
+    AdjAcc acc[P];
+    adj_zero(acc);
+    {
+        double ux[P], uy[P], uz[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            const int o = min(obase + G * p, y.O - 1);
+            ux[p] = y.axes[3 * o];
+            uy[p] = y.axes[3 * o + 1];
+            uz[p] = y.axes[3 * o + 2];
+        }
+        const NearGeom g = near_geom(cx, cy, cz, y.off0, y.off1, y.rc2);
+        ChunkPlan plan;
+        plan.init_range(r.off, r.n_near, r.n_near);
+        stage_prologue(st, plan, y.hi, y.lo, seq);
+        for (int c = 0; c < plan.n_chunks; ++c) {
+            if (!stage_wait(st, plan, c, seq, a.status)) return false;
+            int start, len;
+            bool near;
+            plan.chunk(c, start, len, near);
+            const int s = (seq + c) % kStages;
+            near_convert<NT>(st.hib + s * kCH, st.lob + s * kCH, ed, len);
+            __syncthreads();
+            if (y.near_mode == 2) near_chunk_adj<P, 2>(ed, std4, len, g, ux, uy, uz, acc);
+            else near_chunk_adj<P, 1>(ed, std4, len, g, ux, uy, uz, acc);
+            stage_next(st, plan, y.hi, y.lo, c, seq);
+        }
+        seq += plan.n_chunks;
+    }
+    {
+        float2 ux[PP], uy[PP], uz[PP];
+#pragma unroll
+        for (int j = 0; j < PP; ++j) {
+            const int o0 = min(obase + G * (2 * j), y.O - 1);
+            const int o1 = min(obase + G * (2 * j + 1), y.O - 1);
+            ux[j] = make_float2((float)y.axes[3 * o0], (float)y.axes[3 * o1]);
+            uy[j] = make_float2((float)y.axes[3 * o0 + 1], (float)y.axes[3 * o1 + 1]);
+            uz[j] = make_float2((float)y.axes[3 * o0 + 2], (float)y.axes[3 * o1 + 2]);
+        }
+        const FarGeom g = far_geom(cx, cy, cz, y.off0, y.off1, y.rc2f);
+        ChunkPlan plan;
+        plan.init_range(r.off + r.n_near, 0, r.n_total - r.n_near);
+        stage_prologue(st, plan, y.hi, y.lo, seq);
+        for (int c = 0; c < plan.n_chunks; ++c) {
+            if (!stage_wait(st, plan, c, seq, a.status)) return false;
+            int start, len;
+            bool near;
+            plan.chunk(c, start, len, near);
+            far_chunk_adj<P, true, 16>(st.hib + ((seq + c) % kStages) * kCH, stf, len, g, ux, uy,
+                                       uz, acc);
+            stage_next(st, plan, y.hi, y.lo, c, seq);
+        }
+        seq += plan.n_chunks;
+    }
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        const int o = min(obase + G * p, y.O - 1);
+        adj_finish(acc[p], y.off0, y.off1, y.axes[3 * o], y.axes[3 * o + 1], y.axes[3 * o + 2],
+                   e[p], gr[p]);
+    }
+    return true;
+}
+
+template <int CB, int G, int P, int MINB, bool ADJ>
 __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
     constexpr int NT = CB * G, PP = P / 2;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -94,9 +168,14 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
         frac_to_cart(y.H, (gi + .5) / y.S - r.of[0], (gj + .5) / y.S - r.of[1],
                      (gk + .5) / y.S - r.of[2], cx, cy, cz);
         const int obase = w.z * (G * P) + og;
-
-        // ---- near pairs (FP64)
         double e[P];
+        double gr[ADJ ? P : 1][6];
+        if constexpr (ADJ) {
+            if (!batch_item_adj<CB, G, P>(a, y, r, st, ed, stf, std4, seq, cx, cy, cz, obase, e,
+                                          gr))
+                return;
+        } else {
+        // ---- near pairs (FP64)
         {
             double ux[P], uy[P], uz[P], acc[P][2];
 #pragma unroll
@@ -157,6 +236,7 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
 #pragma unroll
             for (int p = 0; p < P; ++p) e[p] += acc[p];
         }
+        }
         if (cvalid) {
             const long long S3 = (long long)y.S * y.S * y.S;
             const long long cg = ((long long)gi * y.S + gj) * y.S + gk;
@@ -169,6 +249,14 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
                     if (o < y.O) {
                         const long long idx = (long long)o * S3 + cg;
                         y.out[idx] = (float)v;
+                        if (y.out64) y.out64[idx] = v;
+                        if constexpr (ADJ) {
+                            float2 *gd = reinterpret_cast<float2 *>(y.grad + 6 * idx);
+                            const double *gp = gr[2 * j + h];
+                            gd[0] = make_float2((float)gp[0], (float)gp[1]);
+                            gd[1] = make_float2((float)gp[2], (float)gp[3]);
+                            gd[2] = make_float2((float)gp[4], (float)gp[5]);
+                        }
                         if (v > a.band_lo && v < a.band_hi) {
                             const int k = atomicAdd(&a.refine[0], 1);
                             if (k < a.refine_cap) {
@@ -222,16 +310,40 @@ __global__ void batch_refine_kernel(BatchArgs a) {
         }
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
-        if (lane == 0) y.out[idx] = (float)sum;
+        if (lane == 0) {
+            y.out[idx] = (float)sum;
+            if (y.out64) y.out64[idx] = sum;
+        }
     }
 }
 
 // ---------------------------------------------------------------- host side
 
 struct BatchConfig {
-    int shape;   // 0: <16, 8, 4> x 128 threads, 1: <16, 16, 2> x 256 threads (32 directors each)
+    int shape;   // index into the mode's kernel table (batch_kernels)
     int grid;    // resident CTAs (persistent grid)
 };
+
+// CTA shapes the autotuner chooses from; every shape covers a 32-director
+// block (G x P = 32).  Forward: <16, 8, 4> x 128 threads or <16, 16, 2> x 256.
+// Forward + adjoint (9 FP64 sums per director): <16, 16, 2> x 256 or
+// <16, 8, 4> x 128 with fewer CTAs per SM.
+struct BatchKernel {
+    void (*fn)(BatchArgs);
+    int threads;
+    const char *name;
+};
+
+static const BatchKernel kForwardKernels[2] = {
+    {batch_field_kernel<16, 8, 4, 4, false>, 128, "128x4"},
+    {batch_field_kernel<16, 16, 2, 3, false>, 256, "256x2"}};
+static const BatchKernel kAdjointKernels[2] = {
+    {batch_field_kernel<16, 16, 2, 2, true>, 256, "256x2"},
+    {batch_field_kernel<16, 8, 4, 2, true>, 128, "128x4"}};
+
+static const BatchKernel &batch_kernel(bool adj, int shape) {
+    return adj ? kAdjointKernels[shape] : kForwardKernels[shape];
+}
 
 }  // namespace vext
 
@@ -251,6 +363,7 @@ struct vext_batch_s {
     int max_types = 0;
     int64_t poses = 0, list_bytes = 0;
     BatchConfig config{0, 0};
+    bool adj = false;
     float tune_ms[4] = {0, 0, 0, 0};
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
@@ -288,11 +401,8 @@ static int batch_launch(vext_batch b, const BatchConfig &cfg, const int4 *items,
     const size_t smem = batch_smem(b->max_types);
     VEXT_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(int), st));
     VEXT_CUDA(cudaMemsetAsync(b->d_refine, 0, sizeof(int), st));
-    if (cfg.shape == 0) {
-        batch_field_kernel<16, 8, 4, 4><<<cfg.grid, 128, smem, st>>>(a);
-    } else {
-        batch_field_kernel<16, 16, 2, 3><<<cfg.grid, 256, smem, st>>>(a);
-    }
+    const BatchKernel &k = batch_kernel(b->adj, cfg.shape);
+    k.fn<<<cfg.grid, k.threads, smem, st>>>(a);
     VEXT_CUDA(cudaGetLastError());
     if (b->opt.band_hi > b->opt.band_lo) {
         batch_refine_kernel<<<1184, 256, 0, st>>>(a);
@@ -301,11 +411,20 @@ static int batch_launch(vext_batch b, const BatchConfig &cfg, const int4 *items,
     return 0;
 }
 
-extern "C" int vext_batch_create(int n_systems, const vext_system *systems, int size,
-                                 int n_axes, const double *axes, const vext_options *opt,
-                                 float *const *outputs, vext_batch *out) {
+namespace vext {
+
+// Shared by vext_batch_create, vext_batch_create_adjoint and the cached
+// one-system batch of vext_field_adjoint_device (which already holds its
+// system's lock: lock_systems = false).
+int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
+                const double *axes, const vext_options *opt, float *const *outputs,
+                float *const *gradients, double *const *outputs_f64, bool lock_systems,
+                vext_batch *out) {
     if (!out || n_systems < 1 || !systems || !outputs || size < 1 || n_axes < 1 || !axes)
         return fail(VEXT_ERR_ARGUMENT, "bad batch arguments");
+    for (int k = 0; k < n_systems; ++k)
+        if (!systems[k] || !outputs[k] || (gradients && !gradients[k]))
+            return fail(VEXT_ERR_ARGUMENT, "null system or output %d", k);
     *out = nullptr;
     const long long S3 = (long long)size * size * size;
     if (S3 * n_axes >= (1LL << 31) - 1)
@@ -318,6 +437,7 @@ extern "C" int vext_batch_create(int n_systems, const vext_system *systems, int 
     b->size = size;
     b->n_axes = n_axes;
     b->opt = resolve_options(opt);
+    b->adj = gradients != nullptr;
     if (b->opt.mode != VEXT_MODE_MIXED)
         return fail(VEXT_ERR_ARGUMENT, "batched fields run in the mixed mode only");
     int dev = 0;
@@ -332,7 +452,8 @@ extern "C" int vext_batch_create(int n_systems, const vext_system *systems, int 
         System *sys = &systems[k]->sys;
         if (sys->device != dev)
             return fail(VEXT_ERR_ARGUMENT, "system %d lives on another device", k);
-        std::lock_guard<std::mutex> lock(sys->lock);
+        std::unique_lock<std::mutex> lock(sys->lock, std::defer_lock);
+        if (lock_systems) lock.lock();
         RegionSet *rs = nullptr;
         VEXT_TRY(get_field_regions(sys, size, 16, b->opt.r_split, &rs, sys->stream));
         BatchSys &y = hs[k];
@@ -359,6 +480,8 @@ extern "C" int vext_batch_create(int n_systems, const vext_system *systems, int 
         y.nrj = rs->n_rj;
         y.nrk = rs->n_rk;
         y.out = outputs[k];
+        y.grad = gradients ? gradients[k] : nullptr;
+        y.out64 = outputs_f64 ? outputs_f64[k] : nullptr;
         b->max_types = std::max(b->max_types, sys->n_types);
         b->poses += S3 * n_axes;
         b->list_bytes += rs->n_entries * 32;
@@ -390,16 +513,15 @@ extern "C" int vext_batch_create(int n_systems, const vext_system *systems, int 
     VEXT_CUDA(cudaMemset(b->d_status, 0, sizeof(int)));
     // ---- autotune: CTA shape x resident CTAs per SM, on the sampled queue
     const size_t smem = batch_smem(b->max_types);
-    VEXT_CUDA(cudaFuncSetAttribute(batch_field_kernel<16, 8, 4, 4>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    VEXT_CUDA(cudaFuncSetAttribute(batch_field_kernel<16, 16, 2, 3>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int sms = 0, occ0 = 0, occ1 = 0;
+    int sms = 0, occ[2] = {0, 0};
     VEXT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    VEXT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, batch_field_kernel<16, 8, 4, 4>,
-                                                            128, smem));
-    VEXT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, batch_field_kernel<16, 16, 2, 3>,
-                                                            256, smem));
+    for (int k = 0; k < 2; ++k) {
+        const BatchKernel &bk = batch_kernel(b->adj, k);
+        VEXT_CUDA(cudaFuncSetAttribute(bk.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+        VEXT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[k], bk.fn, bk.threads, smem));
+    }
+    const int occ0 = occ[0], occ1 = occ[1];
     if (occ0 < 1 || occ1 < 1) return fail(VEXT_ERR_CAPACITY, "batch kernel does not fit an SM");
     const BatchConfig cands[4] = {{0, sms * occ0}, {0, sms * std::max(1, occ0 / 2)},
                                   {1, sms * occ1}, {1, sms * std::max(1, occ1 / 2)}};
@@ -442,10 +564,37 @@ extern "C" int vext_batch_create(int n_systems, const vext_system *systems, int 
     return 0;
 }
 
+}  // namespace vext
+
+extern "C" int vext_batch_create(int n_systems, const vext_system *systems, int size,
+                                 int n_axes, const double *axes, const vext_options *opt,
+                                 float *const *outputs, vext_batch *out) {
+    return batch_build(n_systems, systems, size, n_axes, axes, opt, outputs, nullptr, nullptr,
+                       true, out);
+}
+
+extern "C" int vext_batch_create_adjoint(int n_systems, const vext_system *systems, int size,
+                                         int n_axes, const double *axes,
+                                         const vext_options *opt, float *const *energies,
+                                         float *const *gradients, vext_batch *out) {
+    if (!gradients) return fail(VEXT_ERR_ARGUMENT, "gradient outputs required");
+    return batch_build(n_systems, systems, size, n_axes, axes, opt, energies, gradients, nullptr,
+                       true, out);
+}
+
+namespace vext {
+
+// Replay on exactly `stream` (0 = the legacy default stream).
+int batch_replay(vext_batch b, cudaStream_t stream) {
+    VEXT_CUDA(cudaGraphLaunch(b->exec, stream));
+    return 0;
+}
+
+}  // namespace vext
+
 extern "C" int vext_batch_run(vext_batch b, void *stream) {
     if (!b) return fail(VEXT_ERR_ARGUMENT, "null batch");
-    VEXT_CUDA(cudaGraphLaunch(b->exec, stream ? (cudaStream_t)stream : b->stream));
-    return 0;
+    return batch_replay(b, stream ? (cudaStream_t)stream : b->stream);
 }
 
 extern "C" int vext_batch_status(vext_batch b) {

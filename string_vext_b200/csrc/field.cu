@@ -401,6 +401,68 @@ __global__ void __launch_bounds__(256) plain_fp64_kernel(FieldArgs a) {
     }
 }
 
+// The plain FP64 forward + adjoint: plain_fp64_kernel plus, per in-cutoff
+// pair off the contact floor, dE/d(r^2) = (-6 c12 i6^2 + 3 c6 i6) i2 and the
+// site gradient 2 dE/d(r^2) (site - x); dE/dc = sum over sites, dE/du =
+// sum o_s x site gradient, projected on the plane normal to u.  Any output
+// may be null ([O][S^3] energies, [O][S^3][6] gradients).
+__global__ void __launch_bounds__(256)
+    plain_fp64_adj_kernel(FieldArgs a, double *e64, double *g64, float *e32, float *g32) {
+    const long long S3 = (long long)a.S * a.S * a.S;
+    const long long n = S3 * a.O;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long c = idx % S3;
+        const int o = (int)(idx / S3);
+        const int gi = (int)(c / ((long long)a.S * a.S)), gj = (int)((c / a.S) % a.S),
+                  gk = (int)(c % a.S);
+        const RegionInfo r = a.regs[region_of(a, gi, gj, gk)];
+        double cx, cy, cz;
+        frac_to_cart(a.H, (gi + .5) / a.S - r.of[0], (gj + .5) / a.S - r.of[1],
+                     (gk + .5) / a.S - r.of[2], cx, cy, cz);
+        const double u[3] = {a.axes[3 * o], a.axes[3 * o + 1], a.axes[3 * o + 2]};
+        double e = 0.0, gc[3] = {0, 0, 0}, gu[3] = {0, 0, 0};
+        for (int s = 0; s < 2; ++s) {
+            const double off = s ? a.off1 : a.off0;
+            const double px = cx + off * u[0], py = cy + off * u[1], pz = cz + off * u[2];
+            double gs[3] = {0, 0, 0};
+            for (int k = 0; k < r.n_total; ++k) {
+                const float4 h = a.hi[r.off + k], l = a.lo[r.off + k];
+                const double dx = px - ((double)h.x + (double)l.x);
+                const double dy = py - ((double)h.y + (double)l.y);
+                const double dz = pz - ((double)h.z + (double)l.z);
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                if (d2 >= a.rc2) continue;
+                const int t = __float_as_int(h.w);
+                const double c12 = a.td[4 * t], c6 = a.td[4 * t + 1], fl = a.td[4 * t + 3];
+                const double s2 = d2 < fl ? fl : d2;
+                const double i2 = 1.0 / s2;
+                const double i6 = i2 * i2 * i2;
+                e += c12 * i6 * i6 - c6 * i6 + a.td[4 * t + 2];
+                if (d2 >= fl) {
+                    const double de = 2.0 * (-6.0 * c12 * i6 * i6 + 3.0 * c6 * i6) * i2;
+                    gs[0] += de * dx;
+                    gs[1] += de * dy;
+                    gs[2] += de * dz;
+                }
+            }
+            for (int k = 0; k < 3; ++k) {
+                gc[k] += gs[k];
+                gu[k] += off * gs[k];
+            }
+        }
+        const double uu = gu[0] * u[0] + gu[1] * u[1] + gu[2] * u[2];
+        const double g[6] = {gc[0], gc[1], gc[2], gu[0] - uu * u[0], gu[1] - uu * u[1],
+                             gu[2] - uu * u[2]};
+        if (e64) e64[idx] = e;
+        if (e32) e32[idx] = (float)e;
+        for (int k = 0; k < 6; ++k) {
+            if (g64) g64[6 * idx + k] = g[k];
+            if (g32) g32[6 * idx + k] = (float)g[k];
+        }
+    }
+}
+
 // ---------------------------------------------------------------- launchers
 
 static size_t near_smem(int n_types) {
@@ -675,6 +737,100 @@ extern "C" int vext_field_device(vext_system h, int size, int n_axes, const doub
     const Options o = resolve_options(opt);
     return field_device(sys, size, n_axes, axes_host, o, orientation_K, energy_f64, marginal_K,
                         site_K, grid, (cudaStream_t)stream, nullptr);
+}
+
+namespace vext {
+
+static int field_adjoint_device(vext_system h, int size, int n_axes, const double *axes,
+                                const Options &o, const vext_options *opt, float *energy,
+                                float *gradient, double *energy_f64, double *gradient_f64,
+                                cudaStream_t stream) {
+    System *sys = &h->sys;
+    if (size < 1 || n_axes < 1 || !axes)
+        return fail(VEXT_ERR_ARGUMENT, "size >= 1, n_axes >= 1 and axes required");
+    const long long S3 = (long long)size * size * size;
+    if (S3 * n_axes * 6 >= (1LL << 40))
+        return fail(VEXT_ERR_CAPACITY, "field too large");
+    for (int k = 0; k < 3 * n_axes; ++k)
+        if (!std::isfinite(axes[k])) return fail(VEXT_ERR_ARGUMENT, "non-finite director");
+    if (o.mode == VEXT_MODE_MIXED) {
+        if (!energy || !gradient)
+            return fail(VEXT_ERR_ARGUMENT, "the mixed adjoint writes float32 energy and gradient");
+        if (gradient_f64)
+            return fail(VEXT_ERR_ARGUMENT, "the FP64 gradient needs an FP64 mode");
+        const bool same = sys->adj_batch && sys->adj_size == size &&
+                          sys->adj_axes.size() == 3 * (size_t)n_axes &&
+                          std::equal(axes, axes + 3 * n_axes, sys->adj_axes.begin()) &&
+                          sys->adj_key[0] == o.r_split && sys->adj_key[1] == o.band_lo &&
+                          sys->adj_key[2] == o.band_hi && sys->adj_energy == energy &&
+                          sys->adj_grad == gradient && sys->adj_energy64 == energy_f64;
+        if (!same) {
+            sys->drop_adjoint_batch();
+            vext_batch b = nullptr;
+            VEXT_TRY(batch_build(1, &h, size, n_axes, axes, opt, &energy, &gradient,
+                                 energy_f64 ? &energy_f64 : nullptr, false, &b));
+            sys->adj_batch = b;
+            sys->adj_size = size;
+            sys->adj_axes.assign(axes, axes + 3 * n_axes);
+            sys->adj_key[0] = o.r_split;
+            sys->adj_key[1] = o.band_lo;
+            sys->adj_key[2] = o.band_hi;
+            sys->adj_energy = energy;
+            sys->adj_grad = gradient;
+            sys->adj_energy64 = energy_f64;
+        }
+        return batch_replay(sys->adj_batch, stream);
+    }
+    if (o.mode != VEXT_MODE_FP64 && o.mode != VEXT_MODE_FP64_PLAIN)
+        return fail(VEXT_ERR_ARGUMENT, "unknown precision mode %d", o.mode);
+    RegionSet *rs = nullptr;
+    VEXT_TRY(get_field_regions(sys, size, 16, 1e30, &rs, stream));
+    VEXT_TRY(ensure_capacity(sys->d_axes, sys->axes_cap, 3 * (size_t)n_axes));
+    VEXT_CUDA(cudaMemcpyAsync(sys->d_axes, axes, sizeof(double) * 3 * n_axes,
+                              cudaMemcpyHostToDevice, stream));
+    const FieldArgs a = make_args(sys, rs, n_axes, sys->d_axes, nullptr);
+    plain_fp64_adj_kernel<<<148 * 16, 256, 0, stream>>>(a, energy_f64, gradient_f64, energy,
+                                                        gradient);
+    VEXT_CUDA(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace vext
+
+extern "C" int vext_field_adjoint_device(vext_system h, int size, int n_axes,
+                                         const double *axes_host, const vext_options *opt,
+                                         float *energy, float *gradient, double *energy_f64,
+                                         double *gradient_f64, void *stream) {
+    if (!h) return fail(VEXT_ERR_ARGUMENT, "null system");
+    System *sys = &h->sys;
+    std::lock_guard<std::mutex> guard(sys->lock);
+    VEXT_CUDA(cudaSetDevice(sys->device));
+    const Options o = resolve_options(opt);
+    return field_adjoint_device(h, size, n_axes, axes_host, o, opt, energy, gradient, energy_f64,
+                                gradient_f64, (cudaStream_t)stream);
+}
+
+extern "C" int vext_field_adjoint(vext_system h, int size, int n_axes, const double *axes,
+                                  const vext_options *opt, float *energy, float *gradient) {
+    if (!h) return fail(VEXT_ERR_ARGUMENT, "null system");
+    if (!energy || !gradient) return fail(VEXT_ERR_ARGUMENT, "energy and gradient required");
+    if (size < 1 || n_axes < 1) return fail(VEXT_ERR_ARGUMENT, "size >= 1 and n_axes >= 1");
+    System *sys = &h->sys;
+    std::lock_guard<std::mutex> guard(sys->lock);
+    VEXT_CUDA(cudaSetDevice(sys->device));
+    const Options o = resolve_options(opt);
+    const size_t n = (size_t)size * size * size * (size_t)n_axes;
+    VEXT_TRY(ensure_capacity(sys->d_f32, sys->f32_cap, n));
+    VEXT_TRY(ensure_capacity(sys->d_g32, sys->g32_cap, 6 * n));
+    cudaStream_t st = sys->stream;
+    VEXT_TRY(field_adjoint_device(h, size, n_axes, axes, o, opt, sys->d_f32, sys->d_g32, nullptr,
+                                  nullptr, st));
+    VEXT_CUDA(cudaMemcpyAsync(energy, sys->d_f32, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    VEXT_CUDA(cudaMemcpyAsync(gradient, sys->d_g32, sizeof(float) * 6 * n,
+                              cudaMemcpyDeviceToHost, st));
+    VEXT_CUDA(cudaStreamSynchronize(st));
+    if (sys->adj_batch && o.mode == VEXT_MODE_MIXED) return vext_batch_status(sys->adj_batch);
+    return check_status(sys, st);
 }
 
 extern "C" int vext_count_pairs(vext_system h, int size, int n_axes, const double *axes,

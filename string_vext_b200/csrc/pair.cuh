@@ -272,4 +272,181 @@ __device__ __forceinline__ void far_chunk(const float4 *hb, const float4 *stf, i
     }
 }
 
+// ------------------------------------------------------------ adjoint
+//
+// Forward + adjoint sums of one pose (center c, unit director u, sites at
+// c + o_s u).  With d0 = x - c and q_s = |d0 - o_s u|^2 = |d0|^2 + o_s^2 -
+// 2 o_s (d0 . u), every pair contributes through fp_s = (dE/dq_s) / 3 =
+// q^-4 (c6 - 2 c12 q^-3)  (zero beyond the cutoff and on the contact floor):
+//   dE/dc = -6 (sum_s H_s - u sum_s o_s F_s)
+//   dE/du = -6 (sum_s o_s H_s) + (terms along u, removed by the tangent
+//           projection),
+// with H_s = sum_x fp_s d0 and F_s = sum_x fp_s.  AdjAcc holds E, H_s, F_s of
+// one director in FP64.
+struct AdjAcc {
+    double e, h[2][3], f[2];
+};
+
+template <int P>
+__device__ __forceinline__ void adj_zero(AdjAcc (&acc)[P]) {
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        acc[p].e = 0.0;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            acc[p].f[q] = 0.0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) acc[p].h[q][k] = 0.0;
+        }
+    }
+}
+
+// Energy and the six gradient components (dE/dc, tangent dE/du) of one
+// director from its sums.
+__device__ __forceinline__ void adj_finish(const AdjAcc &a, double off0, double off1, double ux,
+                                           double uy, double uz, double &e, double (&g)[6]) {
+    const double u[3] = {ux, uy, uz};
+    const double sw = off0 * a.f[0] + off1 * a.f[1];
+    double w[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        g[k] = -6.0 * (a.h[0][k] + a.h[1][k] - u[k] * sw);
+        w[k] = -6.0 * (off0 * a.h[0][k] + off1 * a.h[1][k]);
+    }
+    const double wu = w[0] * u[0] + w[1] * u[1] + w[2] * u[2];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) g[3 + k] = w[k] - wu * u[k];
+    e = a.e;
+}
+
+// FP64 near chunk, forward + adjoint (MODE 1: cutoff test, MODE 2: none);
+// same centre-based q as near_chunk.
+template <int P, int MODE>
+__device__ __forceinline__ void near_chunk_adj(const double *ed, const double *std4, int len,
+                                               const NearGeom &g, const double (&ux)[P],
+                                               const double (&uy)[P], const double (&uz)[P],
+                                               AdjAcc (&acc)[P]) {
+    static_assert(MODE == 1 || MODE == 2, "mixed modes only");
+    const double2 *ed2 = reinterpret_cast<const double2 *>(ed);
+    const double2 *td2 = reinterpret_cast<const double2 *>(std4);
+#pragma unroll 1
+    for (int e = 0; e < len; ++e) {
+        const double2 xy = ed2[2 * e], zt = ed2[2 * e + 1];
+        const int t = (int)zt.y;
+        const double2 cc = td2[2 * t], sh = td2[2 * t + 1];   // (c12, c6), (shift, floor2)
+        const double m2c12 = -2.0 * cc.x;
+        const double dx = xy.x - g.cx, dy = xy.y - g.cy, dz = zt.x - g.cz;
+        const double dd = fma(dx, dx, fma(dy, dy, dz * dz));
+        const double k0 = dd + g.oo0, k1 = dd + g.oo1;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            const double tt = fma(dx, ux[p], fma(dy, uy[p], dz * uz[p]));
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const double d2 = fma(q ? g.m1 : g.m0, tt, q ? k1 : k0);
+                const double s2 = fmax(d2, sh.y);
+                const double i2 = rcp64_nr(s2);
+                const double i6 = i2 * i2 * i2;
+                double en = fma(i6, fma(cc.x, i6, -cc.y), sh.x);
+                double fp = d2 < sh.y ? 0.0 : (i6 * i2) * fma(m2c12, i6, cc.y);
+                if (MODE == 1) {
+                    const bool in = d2 < g.rc2;
+                    en = in ? en : 0.0;
+                    fp = in ? fp : 0.0;
+                }
+                acc[p].e += en;
+                acc[p].h[q][0] = fma(fp, dx, acc[p].h[q][0]);
+                acc[p].h[q][1] = fma(fp, dy, acc[p].h[q][1]);
+                acc[p].h[q][2] = fma(fp, dz, acc[p].h[q][2]);
+                acc[p].f[q] += fp;
+            }
+        }
+    }
+}
+
+// Packed FP32x2 far chunk, forward + adjoint (lanes = two directors).  Per
+// site: n3 = -1/q^3 (hardware reciprocal of -q^3, NEWTON-refined), m = 1/0
+// cutoff mask, n3m = n3 m;  e = n3m (c12 n3m + c6) + m shift;  fp = n3m (2 c12
+// n3m + c6) (n3 q^2) = (dE/dq) / 3.  FP32 partials over FLUSH entries are
+// flushed into the FP64 AdjAcc.
+template <int P, bool NEWTON, int FLUSH>
+__device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *stf, int len,
+                                              const FarGeom &g, const float2 (&ux)[P / 2],
+                                              const float2 (&uy)[P / 2],
+                                              const float2 (&uz)[P / 2], AdjAcc (&acc)[P]) {
+    constexpr int PP = P / 2;
+    const float2 one2 = make_float2(1.f, 1.f);
+#pragma unroll 1
+    for (int e0 = 0; e0 < len; e0 += FLUSH) {
+        float2 fe[PP], fh[PP][2][3], ff[PP][2];
+#pragma unroll
+        for (int j = 0; j < PP; ++j) {
+            fe[j] = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                ff[j][q] = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) fh[j][q][k] = make_float2(0.f, 0.f);
+            }
+        }
+        const int e1 = min(e0 + FLUSH, len);
+#pragma unroll 1
+        for (int e = e0; e < e1; ++e) {
+            const float4 h = hb[e];
+            const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, -)
+            const float dx = h.x - g.cx, dy = h.y - g.cy, dz = h.z - g.cz;
+            const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float2 k0 = make_float2(dd + g.oo0, dd + g.oo0),
+                         k1 = make_float2(dd + g.oo1, dd + g.oo1);
+            const float2 dx2 = make_float2(dx, dx), dy2 = make_float2(dy, dy),
+                         dz2 = make_float2(dz, dz);
+            const float2 c12 = make_float2(tp.x, tp.x), c6 = make_float2(tp.y, tp.y),
+                         sh = make_float2(tp.z, tp.z),
+                         c12x2 = make_float2(2.f * tp.x, 2.f * tp.x);
+#pragma unroll
+            for (int j = 0; j < PP; ++j) {
+                const float2 t =
+                    __ffma2_rn(dx2, ux[j], __ffma2_rn(dy2, uy[j], __fmul2_rn(dz2, uz[j])));
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const float2 d2 = __ffma2_rn(q ? g.m1 : g.m0, t, q ? k1 : k0);
+                    const float2 dsq = __fmul2_rn(d2, d2);
+                    const float2 d6 = __fmul2_rn(dsq, d2);
+                    float r0, r1;
+                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(-d6.x));
+                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r1) : "f"(-d6.y));
+                    float2 n3 = make_float2(r0, r1);
+                    if (NEWTON) n3 = __ffma2_rn(n3, __ffma2_rn(d6, n3, one2), n3);
+                    const float2 m = make_float2(set_lt(d2.x, g.rc2f), set_lt(d2.y, g.rc2f));
+                    const float2 n3m = __fmul2_rn(n3, m);
+                    fe[j] = __ffma2_rn(n3m, __ffma2_rn(c12, n3m, c6), fe[j]);
+                    fe[j] = __ffma2_rn(m, sh, fe[j]);
+                    const float2 ea = __fmul2_rn(n3m, __ffma2_rn(c12x2, n3m, c6));
+                    const float2 fp = __fmul2_rn(ea, __fmul2_rn(n3, dsq));
+                    fh[j][q][0] = __ffma2_rn(fp, dx2, fh[j][q][0]);
+                    fh[j][q][1] = __ffma2_rn(fp, dy2, fh[j][q][1]);
+                    fh[j][q][2] = __ffma2_rn(fp, dz2, fh[j][q][2]);
+                    ff[j][q] = __fadd2_rn(fp, ff[j][q]);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < PP; ++j) {
+            AdjAcc &a0 = acc[2 * j], &a1 = acc[2 * j + 1];
+            a0.e += (double)fe[j].x;
+            a1.e += (double)fe[j].y;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                a0.f[q] += (double)ff[j][q].x;
+                a1.f[q] += (double)ff[j][q].y;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    a0.h[q][k] += (double)fh[j][q][k].x;
+                    a1.h[q][k] += (double)fh[j][q][k].y;
+                }
+            }
+        }
+    }
+}
+
 }  // namespace vext

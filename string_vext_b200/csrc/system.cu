@@ -410,8 +410,17 @@ int check_status(System *sys, cudaStream_t stream) {
     return fail(VEXT_ERR_CUDA, "device list build inconsistency (status %d)", h);
 }
 
+void System::drop_adjoint_batch() {
+    if (adj_batch) vext_batch_destroy(adj_batch);
+    adj_batch = nullptr;
+    adj_size = 0;
+    adj_axes.clear();
+}
+
 System::~System() {
+    drop_adjoint_batch();   // it points into the region sets
     for (RegionSet *rs : sets) delete rs;
+    cudaFree(d_g32);
     cudaFree(d_frac);
     cudaFree(d_type);
     cudaFree(d_tf);
@@ -573,6 +582,7 @@ extern "C" int vext_system_invalidate(vext_system h) {
     if (!h) return fail(VEXT_ERR_ARGUMENT, "null system");
     std::lock_guard<std::mutex> guard(h->sys.lock);
     for (RegionSet *rs : h->sys.sets) rs->stale = true;
+    h->sys.drop_adjoint_batch();
     return 0;
 }
 

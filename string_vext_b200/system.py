@@ -126,6 +126,32 @@ class VextSystem:
                                                _lib.ptr(out_energy), _lib.ptr(out_marginal),
                                                _lib.ptr(out_site), _lib.ptr(out_grid), handle))
 
+    def field_adjoint(self, size: int, axes, mode: int = _lib.VEXT_MODE_MIXED, **opts):
+        """Forward + adjoint over the field poses (host arrays).  Returns the
+        float32 energy [O, S, S, S] and gradient [O, S, S, S, 6] = (dE/dcenter,
+        dE/du projected on the plane normal to u)."""
+        axes = _c(axes)
+        n_axes = len(axes)
+        energy = np.empty((n_axes, size, size, size), np.float32)
+        grad = np.empty((n_axes, size, size, size, 6), np.float32)
+        opt = _lib.options(mode, **opts)
+        _lib.check(self._lib.vext_field_adjoint(self.handle, size, n_axes, _lib.ptr(axes),
+                                                ctypes.byref(opt), _lib.ptr(energy),
+                                                _lib.ptr(grad)))
+        return energy, grad
+
+    def field_adjoint_device(self, size: int, axes, energy=None, gradient=None,
+                             energy_f64=None, gradient_f64=None,
+                             mode: int = _lib.VEXT_MODE_MIXED, stream=None, **opts) -> None:
+        """Device-pointer variant (CUDA tensors, [O, S, S, S] and [O, S, S, S, 6]);
+        the mixed mode writes float32 outputs, the FP64 modes any of the four."""
+        axes = _c(axes)
+        opt = _lib.options(mode, **opts)
+        handle = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        _lib.check(self._lib.vext_field_adjoint_device(
+            self.handle, size, len(axes), _lib.ptr(axes), ctypes.byref(opt), _lib.ptr(energy),
+            _lib.ptr(gradient), _lib.ptr(energy_f64), _lib.ptr(gradient_f64), handle))
+
     # ------------------------------------------------------------------ poses
     def pose_energy_grad(self, centers, quats, mode: int = _lib.VEXT_MODE_MIXED,
                          grad: bool = True, **opts):
@@ -161,18 +187,28 @@ class VextBatch:
     (``vext_batch_create``).  ``outputs`` are CUDA float32 tensors
     [n_axes, S, S, S], one per system; ``run()`` replays the graph."""
 
-    def __init__(self, systems, size: int, axes, outputs, **opts):
+    def __init__(self, systems, size: int, axes, outputs, gradients=None, **opts):
         self._lib = _lib.load()
         self.systems = list(systems)           # kept alive: the batch points into them
         self.outputs = list(outputs)
+        self.gradients = list(gradients) if gradients is not None else None
         self.axes = _c(axes)
         handles = (ctypes.c_void_p * len(self.systems))(*[s.handle.value for s in self.systems])
         outs = (ctypes.c_void_p * len(self.outputs))(*[o.data_ptr() for o in self.outputs])
         opt = _lib.options(_lib.VEXT_MODE_MIXED, **opts)
         handle = ctypes.c_void_p()
-        _lib.check(self._lib.vext_batch_create(len(self.systems), handles, size, len(self.axes),
-                                               _lib.ptr(self.axes), ctypes.byref(opt), outs,
-                                               ctypes.byref(handle)))
+        if self.gradients is None:
+            _lib.check(self._lib.vext_batch_create(len(self.systems), handles, size,
+                                                   len(self.axes), _lib.ptr(self.axes),
+                                                   ctypes.byref(opt), outs,
+                                                   ctypes.byref(handle)))
+        else:
+            grads = (ctypes.c_void_p * len(self.gradients))(
+                *[g.data_ptr() for g in self.gradients])
+            _lib.check(self._lib.vext_batch_create_adjoint(len(self.systems), handles, size,
+                                                           len(self.axes), _lib.ptr(self.axes),
+                                                           ctypes.byref(opt), outs, grads,
+                                                           ctypes.byref(handle)))
         self.handle = handle
 
     def run(self, stream=None) -> None:
@@ -187,8 +223,11 @@ class VextBatch:
         d, e = ctypes.c_int(), ctypes.c_int()
         _lib.check(self._lib.vext_batch_info(self.handle, ctypes.byref(a), ctypes.byref(b),
                                              ctypes.byref(c), ctypes.byref(d), ctypes.byref(e)))
+        adj = self.gradients is not None
+        shapes = ("256x2 dirs", "128x4 dirs") if adj else ("128x4 dirs", "256x2 dirs")
         return {"work_items": a.value, "poses": b.value, "list_bytes": c.value,
-                "shape": d.value, "grid": e.value}
+                "shape": d.value, "cta_shape": shapes[d.value], "grid": e.value,
+                "adjoint": adj}
 
     def close(self) -> None:
         if getattr(self, "handle", None):

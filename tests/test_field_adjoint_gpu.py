@@ -1,0 +1,171 @@
+"""Forward + adjoint over the field poses (energy, dE/d(center), tangent
+dE/d(director) at every grid center x director) through the C ABI, against
+the FP64 oracle's analytic gradient and against central finite differences of
+the FP64 oracle energy.
+
+Tolerances: the plain FP64 kernel agrees with the oracle to 1e-10 relative
+(energy, floor 1 K) and 1e-9 relative (gradient norm, floor 1 K/A); the mixed
+kernel keeps the energy bar on its FP64 energy output (1e-4 K absolute where
+E <= 0, 1e-6 relative above; the float32 output is its rounding) and its
+gradient agrees with the oracle and with central differences (h = 1e-4 A,
+1e-4 rad) to 1e-5 relative.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle
+from string_vext_b200 import _lib, synth
+from string_vext_b200.orientation import normalized_directors, regular_pose_grid
+from string_vext_b200.system import VextBatch, VextSystem
+
+pytestmark = pytest.mark.gpu
+
+FP64 = _lib.VEXT_MODE_FP64
+MIXED = _lib.VEXT_MODE_MIXED
+
+
+def field_poses(case, size, n_axes=64):
+    """Cartesian centers and directors of every pose in [O][S^3] order."""
+    frac, axes = regular_pose_grid(size, n_axes)
+    axes = normalized_directors(axes)
+    cart = frac @ np.asarray(case["cell"], dtype=float)
+    centers = np.broadcast_to(cart[None], (n_axes,) + cart.shape).reshape(-1, 3)
+    dirs = np.broadcast_to(axes[:, None, :], (n_axes, len(cart), 3)).reshape(-1, 3)
+    return axes, np.ascontiguousarray(centers), np.ascontiguousarray(dirs)
+
+
+def oracle_field_adjoint(case, size, n_axes=64):
+    axes, centers, dirs = field_poses(case, size, n_axes)
+    e, gc, gu = oracle.pose_energy_grad(case, centers, dirs)
+    gu_t = gu - (gu * dirs).sum(1)[:, None] * dirs
+    shape = (n_axes, size, size, size)
+    return axes, e.reshape(shape), np.concatenate([gc, gu_t], 1).reshape(shape + (6,))
+
+
+def grad_rel(g, ref):
+    """Per-pose relative error of the 6-vector gradient (floor 1 K/A)."""
+    diff = np.linalg.norm(g - ref, axis=-1)
+    return diff / np.maximum(np.linalg.norm(ref, axis=-1), 1.0)
+
+
+def run_device(system, size, axes, mode, energy64=False, grad64=False):
+    n = len(axes)
+    shape = (n, size, size, size)
+    e = torch.empty(shape, dtype=torch.float32, device="cuda")
+    g = torch.empty(shape + (6,), dtype=torch.float32, device="cuda")
+    e64 = torch.empty(shape, dtype=torch.float64, device="cuda") if energy64 else None
+    g64 = torch.empty(shape + (6,), dtype=torch.float64, device="cuda") if grad64 else None
+    system.field_adjoint_device(size, axes, e, g, e64, g64, mode=mode)
+    torch.cuda.synchronize()
+    out = [e.cpu().numpy(), g.cpu().numpy()]
+    out += [t.cpu().numpy() for t in (e64, g64) if t is not None]
+    return out
+
+
+@pytest.mark.parametrize("maker,size", [(synth.small_field, 4), (synth.full_field, 3),
+                                        (synth.skewed_field, 3)])
+def test_fp64_and_mixed_adjoint_match_oracle(maker, size):
+    case = maker()
+    axes, e_ref, g_ref = oracle_field_adjoint(case, size)
+    with VextSystem(case) as system:
+        e32, g32, e64, g64 = run_device(system, size, axes, FP64, energy64=True, grad64=True)
+        me, mg, me64 = run_device(system, size, axes, MIXED, energy64=True)
+    assert (np.abs(e64 - e_ref) / np.maximum(np.abs(e_ref), 1)).max() < 1e-10
+    assert grad_rel(g64, g_ref).max() < 1e-9
+    np.testing.assert_array_equal(e32, e64.astype(np.float32))
+    np.testing.assert_array_equal(g32, g64.astype(np.float32))
+    np.testing.assert_array_equal(me, me64.astype(np.float32))
+    neg = e_ref <= 0
+    if neg.any():
+        assert np.abs(me64 - e_ref)[neg].max() < 1e-4
+    if (~neg).any():
+        assert (np.abs(me64 - e_ref) / np.maximum(np.abs(e_ref), 1))[~neg].max() < 1e-6
+    assert grad_rel(mg.astype(np.float64), g_ref).max() < 1e-5
+
+
+def test_mixed_gradient_matches_central_differences():
+    """dE/dc and the tangent dE/du of accessible poses (E < 0) against central
+    differences of the FP64 oracle energy, h = 1e-4 A and 1e-4 rad."""
+    case = synth.small_field()
+    size = 6
+    axes, centers, dirs = field_poses(case, size)
+    with VextSystem(case) as system:
+        me, mg = run_device(system, size, axes, MIXED)
+    e = me.reshape(-1)
+    g = mg.reshape(-1, 6).astype(np.float64)
+    pick = np.flatnonzero(e < 0)
+    assert len(pick) >= 32
+    pick = pick[np.linspace(0, len(pick) - 1, 32).astype(int)]
+    c, u = centers[pick], dirs[pick]
+    h = 1e-4
+    fd = np.zeros((len(pick), 6))
+    for k in range(3):
+        step = np.zeros(3)
+        step[k] = h
+        ep, _, _ = oracle.pose_energy_grad(case, c + step, u)
+        em, _, _ = oracle.pose_energy_grad(case, c - step, u)
+        fd[:, k] = (ep - em) / (2 * h)
+    # tangent basis e1, e2 normal to u; rotate u by +-h about each
+    ref = np.where(np.abs(u[:, :1]) < 0.9, [[1.0, 0, 0]], [[0, 1.0, 0]])
+    e1 = np.cross(u, ref)
+    e1 /= np.linalg.norm(e1, axis=1, keepdims=True)
+    e2 = np.cross(u, e1)
+    for basis in (e1, e2):
+        up = np.cos(h) * u + np.sin(h) * basis
+        um = np.cos(h) * u - np.sin(h) * basis
+        ep, _, _ = oracle.pose_energy_grad(case, c, up)
+        em, _, _ = oracle.pose_energy_grad(case, c, um)
+        d_fd = (ep - em) / (2 * h)
+        d_an = (g[pick, 3:] * basis).sum(1)
+        scale = np.maximum(np.linalg.norm(g[pick, 3:], axis=1), 1.0)
+        assert (np.abs(d_an - d_fd) / scale).max() < 1e-5
+    gc = g[pick, :3]
+    scale = np.maximum(np.linalg.norm(fd[:, :3], axis=1), 1.0)
+    assert (np.linalg.norm(gc - fd[:, :3], axis=1) / scale).max() < 1e-5
+
+
+def test_adjoint_batch_matches_single_fields_and_host_entry():
+    cases = synth.batch_frameworks(2) + [synth.small_field()]
+    size = 5
+    _, axes = regular_pose_grid(size, 64)
+    axes = normalized_directors(axes)
+    systems = [VextSystem(c) for c in cases]
+    shape = (64, size, size, size)
+    outs = [torch.full(shape, -1.0, dtype=torch.float32, device="cuda") for _ in systems]
+    grads = [torch.full(shape + (6,), -1.0, dtype=torch.float32, device="cuda")
+             for _ in systems]
+    batch = VextBatch(systems, size, axes, outs, gradients=grads)
+    assert batch.info()["adjoint"]
+    for _ in range(2):
+        batch.run()
+        batch.check()
+        torch.cuda.synchronize()
+        for system, out, grad in zip(systems, outs, grads):
+            e, g = system.field_adjoint(size, axes)
+            np.testing.assert_array_equal(out.cpu().numpy(), e)
+            np.testing.assert_array_equal(grad.cpu().numpy(), g)
+            de, dg = run_device(system, size, axes, MIXED)
+            np.testing.assert_array_equal(de, e)
+            np.testing.assert_array_equal(dg, g)
+    batch.close()
+    for s in systems:
+        s.close()
+
+
+def test_adjoint_rejects_bad_arguments():
+    case = synth.small_field()
+    _, axes = regular_pose_grid(4, 64)
+    axes = normalized_directors(axes)
+    with VextSystem(case) as system:
+        e = torch.empty((64, 4, 4, 4), dtype=torch.float32, device="cuda")
+        g64 = torch.empty((64, 4, 4, 4, 6), dtype=torch.float64, device="cuda")
+        with pytest.raises(_lib.VextError):
+            system.field_adjoint_device(4, axes, e, None)          # mixed needs both outputs
+        g = torch.empty((64, 4, 4, 4, 6), dtype=torch.float32, device="cuda")
+        with pytest.raises(_lib.VextError):
+            system.field_adjoint_device(4, axes, e, g, None, g64)   # FP64 gradient: FP64 modes
+        bad = axes.copy()
+        bad[0, 0] = np.nan
+        with pytest.raises(_lib.VextError):
+            system.field_adjoint_device(4, bad, e, g)
