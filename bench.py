@@ -1,19 +1,22 @@
-"""Benchmark: Vext pose evaluations/s on the full-size field workload.
+"""Benchmark: Vext pose evaluations/s (forward + adjoint) on the full-size field.
 
 Workload (default ``full_field``): 37 x 37 x 3.6 A layered cell (gamma
 119.993), 600 seeded synthetic atoms, two-site guest 85 K / 3.685 A / bond
 1.33 A, cutoff 12.8 A, 60^3 grid x 64 Fibonacci directors = 13,824,000 poses
-per field.  One step = one complete field: region-list build + pair kernel +
-FP64 refinement + float32 epilogue, inputs resident in HBM.
+per field.  One step = the energy, dE/d(center) and tangent dE/d(director)
+of every pose (one replay of the one-system batched forward + adjoint
+kernel), region lists and outputs resident in HBM.
 
 Our arm prints one JSON line with: value (poses/s over all ranks, device time
-from CUDA events, max over ranks), e2e (the public host C-ABI call:
-system upload + field + float32 download), roofline of the pair kernel
-against the measured FP32 FFMA peak of this GPU, the FP64 GPU oracle kernel's
-throughput and the error of the mixed-precision result against it, the
-forward+adjoint pose throughput, clocks sampled during the timed region, and
-a CPU baseline (the reference kernel compiled from its source, driven by the
-restated reference driver, on a bounded sample of the same field).
+from CUDA events, max over ranks), e2e (the public host C-ABI call
+vext_field_adjoint: directors up, float32 energy + gradient down into pinned
+host memory), roofline of the fused pair kernel against the measured FP32
+FFMA peak of this GPU, the forward-only field (list build + pair kernels +
+epilogue, with the far kernel's roofline), the plain and tiled FP64 GPU
+kernels and the error of the mixed result against FP64, the random-pose
+forward+adjoint path, the 100-field batches, clocks sampled during the timed
+region, and a CPU baseline (the reference kernel compiled from its source,
+driven by the restated reference driver, on a bounded sample of the field).
 
 ``--impl reference`` times that reference CPU path alone (all host cores,
 rank 0 only) on the same metric.
@@ -21,6 +24,7 @@ rank 0 only) on the same metric.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -41,6 +45,9 @@ METRIC = "Vext pose evals/s at <=1e-4 K vs FP64, fwd+adjoint evals/s; % FP32 pea
 # dram__bytes_read.sum + dram__bytes_write.sum of one field_far_kernel launch on
 # full_field, from an ncu capture (--set full) of `bench.py --profile field`.
 FAR_DRAM_BYTES_FULL_FIELD = 741_898_752 + 101_475_584
+# the same for one forward + adjoint batch_field_kernel launch on full_field
+# (`bench.py --profile adjoint`); None until captured.
+ADJ_DRAM_BYTES_FULL_FIELD = None
 CPU_CENTERS_PER_CORE_S = 900.0   # reference driver throughput estimate used to size the sample
 
 
@@ -77,7 +84,8 @@ def cpu_model():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons of one GPU every 200 ms."""
+    """nvidia-smi clocks/throttle reasons of one GPU every 100 ms (samples
+    taken before the timed region starts are dropped)."""
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -91,10 +99,14 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            deadline = time.time() + 5.0      # sampling must be live before timing starts
+            while not self.rows and time.time() < deadline and self.proc.poll() is None:
+                time.sleep(0.02)
+            self.rows.clear()
         except OSError:
             self.proc = None
         return self
@@ -137,14 +149,15 @@ def cpu_reference_sample(case, size, n_axes, seconds_target, processes):
                                          CPU_CENTERS_PER_CORE_S * processes * seconds_target)))
     stride = max(1, len(centers) // n_sample)
     sample = centers[::stride][:n_sample]
-    energy, wall, used = oracle.reference_field_parallel(case, sample, axes, library=library,
-                                                         processes=processes, symbol=symbol)
+    energy, wall, used, compute = oracle.reference_field_parallel(
+        case, sample, axes, library=library, processes=processes, symbol=symbol)
     poses = len(sample) * n_axes
-    return {"value": poses / wall, "unit": "poses/s", "cores": used, "kind": kind,
+    return {"value": poses / compute, "unit": "poses/s", "cores": used, "kind": kind,
             "sample": f"{len(sample)} of {len(centers)} grid centers (stride {stride}) x "
-                      f"{n_axes} directors, {processes} spawn processes, kd-tree query + "
-                      f"kernel, {cpu_model()}",
-            "seconds": wall, "poses": poses}
+                      f"{n_axes} directors (forward energies only), {used} spawn processes; "
+                      f"time = slowest worker's kd-tree query + kernel ({compute:.2f} s; "
+                      f"{wall:.2f} s with process start), {cpu_model()}",
+            "seconds": compute, "poses": poses}
 
 
 def run_reference(args, rank, world):
@@ -153,8 +166,10 @@ def run_reference(args, rank, world):
     case, size = workload(args.workload)
     cores = host_cores()
     values = []
+    # each step a bounded sample: about two minutes of CPU work over the whole run
+    per_step = max(0.5, min(args.cpu_seconds, 120.0 / (args.warmup + args.steps)))
     for step in range(args.warmup + args.steps):
-        res = cpu_reference_sample(case, size, 64, args.cpu_seconds, cores)
+        res = cpu_reference_sample(case, size, 64, per_step, cores)
         if step >= args.warmup:
             values.append(res)
     value = sum(r["poses"] for r in values) / sum(r["seconds"] for r in values)
@@ -187,6 +202,19 @@ def error_stats(mixed, exact):
             "passed": bool((diff[neg] < 1e-4).all() and (rel[~neg] < 1e-6).all())}
 
 
+def timed_region(fn, steps, stream):
+    """CUDA-event time (ms) of `steps` calls of fn on `stream`."""
+    import torch
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -201,116 +229,67 @@ def run_ours(args, rank, world, local_rank):
     axes = normalized_directors(axes)
     n_axes = len(axes)
     poses = size ** 3 * n_axes
+    shape = (n_axes, size, size, size)
     stream = torch.cuda.Stream(device)
-    out = torch.empty((n_axes, size, size, size), dtype=torch.float32, device=device)
+    energy = torch.empty(shape, dtype=torch.float32, device=device)
+    grad = torch.empty(shape + (6,), dtype=torch.float32, device=device)
     system = VextSystem(case)
 
     pairs, far_pairs = system.count_pairs(size, axes)
     pipes = _lib.measure_pipes()
     peak = 2.0 * max(pipes["ffma_per_s"], pipes["ffma2_fma_per_s"])   # FLOP/s, FMA = 2
 
+    # ---- headline: forward + adjoint of every pose, one-system batched kernel
+    t0 = time.perf_counter()
+    system.field_adjoint_device(size, axes, energy, grad, stream=stream)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+
     def step():
-        system.invalidate()
-        system.field_device(size, axes, out, stream=stream)
-        return system.last_timings()
+        system.field_adjoint_device(size, axes, energy, grad, stream=stream)
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    timings = []
     with ClockSampler(local_rank) as clocks:
-        torch.cuda.synchronize()
-        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        start.record(stream)
-        for _ in range(args.steps):
-            timings.append(step())
-        stop.record(stream)
-        torch.cuda.synchronize()
-    ms_total = start.elapsed_time(stop)
+        ms_total = timed_region(step, args.steps, stream)
     if world > 1:
         t = torch.tensor([ms_total], device=device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_total = float(t.item())
     ms_step = ms_total / args.steps
     value = world * poses * args.steps / (ms_total * 1e-3)
-    near_ms = statistics.mean(t["near_ms"] for t in timings)
-    far_ms = statistics.mean(t["far_ms"] for t in timings)
-    list_ms = statistics.mean(t["list_ms"] for t in timings)
-    epi_ms = statistics.mean(t["epilogue_ms"] for t in timings)
-    achieved_far = far_pairs * FLOP_FWD / (far_ms * 1e-3)
-    achieved_pairs = pairs * FLOP_FWD / ((near_ms + far_ms) * 1e-3)
+    achieved = pairs * FLOP_FWD_ADJ / (ms_step * 1e-3)
 
-    # e2e through the public host API: system upload + field + float32 download
+    # ---- e2e through the public host entry (vext_field_adjoint): directors
+    # up, float32 energy + gradient down into pinned host buffers, every call
+    h_energy = torch.empty(shape, dtype=torch.float32, pin_memory=True)
+    h_grad = torch.empty(shape + (6,), dtype=torch.float32, pin_memory=True)
+    lib = _lib.load()
+    opt = _lib.options()
+
+    def e2e_call():
+        _lib.check(lib.vext_field_adjoint(system.handle, size, n_axes, _lib.ptr(axes),
+                                          ctypes.byref(opt), _lib.ptr(h_energy),
+                                          _lib.ptr(h_grad)))
+
+    e2e_call()
     e2e_times = []
-    h2d = d2h = 0
-    for i in range(max(2, args.steps // 2) + 1):
-        torch.cuda.synchronize()
+    for _ in range(max(3, min(args.steps, 10))):
         t0 = time.perf_counter()
-        with VextSystem(case) as sys_e2e:
-            res = sys_e2e.field(size, axes)
-        dt = time.perf_counter() - t0
-        if i:
-            e2e_times.append(dt)
-        h2d = (case["frame_frac"].nbytes + case["frame_sigma"].nbytes
-               + case["frame_epsilon"].nbytes + axes.nbytes + 9 * 8)
-        d2h = res["orientation_K"].nbytes
+        e2e_call()
+        e2e_times.append(time.perf_counter() - t0)
     e2e_value = world * poses / statistics.median(e2e_times)
+    h2d, d2h = axes.nbytes, h_energy.numel() * 4 + h_grad.numel() * 4
+    del h_energy, h_grad
 
     extra = {}
     if rank == 0:
-        # FP64 GPU kernels: the tiled FP64 oracle kernel and the plain
-        # one-thread-per-pose FP64 baseline (both one field per launch)
-        exact = system.field(size, axes, mode=_lib.VEXT_MODE_FP64, energy=True,
-                             orientation=False)["energy"]
-        fp64 = {}
-        for label, mode in (("fp64_tiled", _lib.VEXT_MODE_FP64),
-                            ("fp64_plain", _lib.VEXT_MODE_FP64_PLAIN)):
-            times = []
-            for _ in range(2):
-                system.invalidate()
-                torch.cuda.synchronize()
-                system.field(size, axes, mode=mode, orientation=False)
-                st = system.last_stats
-                times.append(st["kernel_ms"] + st["list_build_ms"] + st["epilogue_ms"])
-            fp64[label] = {"value": poses / (min(times) * 1e-3), "unit": "poses/s",
-                           "ms_per_field": min(times)}
-        extra["fp64_kernels"] = fp64
-        extra["speedup_vs_fp64_plain"] = fp64["fp64_plain"]["ms_per_field"] / ms_step
-        extra["speedup_vs_fp64_tiled"] = fp64["fp64_tiled"]["ms_per_field"] / ms_step
-        mixed = system.field(size, axes, energy=True, orientation=False)
-        stats = system.last_stats
-        extra["error_vs_fp64"] = error_stats(mixed["energy"], exact)
-        extra["refined_poses"] = stats["refined_poses"]
-        extra["list_entries"] = stats["list_entries"]
-        extra["near_entries"] = stats["near_entries"]
-        del exact, mixed
-        # forward + adjoint on a random pose batch of the same framework
-        n_pose = 1 << 20
-        rng = np.random.default_rng(9)
-        cart = torch.tensor(rng.random((n_pose, 3)) @ case["cell"], device=device)
-        q = torch.tensor(rng.normal(size=(n_pose, 4)), device=device)
-        e = torch.empty(n_pose, dtype=torch.float64, device=device)
-        gc = torch.empty((n_pose, 3), dtype=torch.float64, device=device)
-        gq = torch.empty((n_pose, 4), dtype=torch.float64, device=device)
-        for _ in range(2):
-            system.pose_energy_grad_device(cart, q, e, gc, gq, stream=stream)
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        reps = 3
-        for _ in range(reps):
-            system.pose_energy_grad_device(cart, q, e, gc, gq, stream=stream)
-        b.record(stream)
-        torch.cuda.synchronize()
-        adj_ms = a.elapsed_time(b) / reps
-        extra["fwd_adjoint"] = {"value": n_pose / (adj_ms * 1e-3), "unit": "poses/s",
-                                "poses": n_pose, "workload": "random poses, same framework",
-                                "flop_per_pair": FLOP_FWD_ADJ}
-        del cart, q, e, gc, gq
-        if not args.no_batch:
-            extra["batch"] = bench_batch(args, size, axes, device, stream)
+        extra.update(secondary_measurements(args, system, case, size, axes, poses, pairs,
+                                            far_pairs, peak, stream, device, ms_step, energy,
+                                            grad))
     if world > 1:
         dist.barrier()
     if rank != 0:
@@ -319,47 +298,164 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_cpu:
         cpu = cpu_reference_sample(case, size, n_axes, args.cpu_seconds, host_cores())
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
-    clock = clocks.summary()
     line = {"metric": METRIC, "value": value, "unit": "poses/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32x2+f64 (pairs < 6 A in FP64, beyond in packed FP32, FP64 refinement band)",
+            "dtype": "f32x2+f64 (pairs < 6 A in FP64, beyond in packed FP32 with FP64-flushed "
+                     "partial sums; FP64 energy refinement band)",
             "data": "synthetic", "config": config_of(args.workload, size),
+            "step": "forward + adjoint of every pose: energy, dE/d(center), tangent dE/du; "
+                    "region lists resident (built once per framework, reported as setup)",
             "e2e": {"value": e2e_value, "unit": "poses/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "path": "vext_system_create + vext_field "
-                    "(host buffers) + vext_system_destroy"},
-            "gpu_launches": args.steps * 7,
-            "step_breakdown_ms": {"list_build": list_ms, "near_pairs_fp64": near_ms,
-                                  "far_pairs_fp32x2": far_ms, "refine_epilogue": epi_ms},
-            "roofline": {"bound": "fp32", "kernel": "field_far_kernel<16,8,4,4> (default variant)",
-                         "achieved": achieved_far / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
-                         "frac": achieved_far / peak,
+                    "d2h_bytes_per_step": d2h,
+                    "path": "vext_field_adjoint (host pinned float32 energy + gradient)"},
+            "gpu_launches": args.steps * 2,
+            "setup_s": setup_s,
+            "roofline": {"bound": "fp32",
+                         "kernel": "batch_field_kernel<adjoint> (fused FP64 near + FP32x2 far)",
+                         "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
+                         "frac": achieved / peak,
                          "peak_source": "measured on this GPU: max(FFMA, FFMA2) FMA rate x 2 "
-                                        "(vext_measure_pipes); MEASURED_PEAKS.json has no FP32 figure",
-                         "algorithmic": f"{far_pairs} far in-cutoff pairs x {FLOP_FWD} FLOP per field",
-                         "traffic": (FAR_DRAM_BYTES_FULL_FIELD
+                                        "(vext_measure_pipes); MEASURED_PEAKS.json has no FP32 "
+                                        "figure",
+                         "algorithmic": f"{pairs} in-cutoff pairs x {FLOP_FWD_ADJ} FLOP "
+                                        "(forward + adjoint) per field",
+                         "traffic": (ADJ_DRAM_BYTES_FULL_FIELD
                                      if args.workload == "full_field" else None),
                          "traffic_unit": "bytes per launch (ncu dram__bytes_read+write)",
-                         "both_pair_kernels": {"achieved": achieved_pairs / 1e12,
-                                               "frac": achieved_pairs / peak,
-                                               "algorithmic": f"{pairs} in-cutoff pairs x {FLOP_FWD} FLOP"},
                          "pipes": pipes},
-            "clocks": clock, "cpu_baseline": cpu}
+            "clocks": clocks.summary(), "cpu_baseline": cpu}
     line.update(extra)
     print(json.dumps(line))
 
 
-def bench_batch(args, size, axes, device, stream):
+def secondary_measurements(args, system, case, size, axes, poses, pairs, far_pairs, peak,
+                           stream, device, ms_adj, energy, grad):
+    """Forward-only field, FP64 baselines, error against FP64, pose path and
+    the 100-field batches (rank 0)."""
+    import torch
+    from string_vext_b200 import _lib
+    n_axes = len(axes)
+    shape = (n_axes, size, size, size)
+    out = {}
+    # forward only: per-field near/far kernels, region lists rebuilt every step
+    fwd_out = torch.empty(shape, dtype=torch.float32, device=device)
+    timings = []
+
+    def fwd_step():
+        system.invalidate()
+        system.field_device(size, axes, fwd_out, stream=stream)
+        timings.append(system.last_timings())
+
+    for _ in range(args.warmup):
+        fwd_step()
+    timings.clear()
+    n_fwd = max(3, min(args.steps, 10))
+    fwd_ms = timed_region(fwd_step, n_fwd, stream) / n_fwd
+    near_ms = statistics.mean(t["near_ms"] for t in timings)
+    far_ms = statistics.mean(t["far_ms"] for t in timings)
+    list_ms = statistics.mean(t["list_ms"] for t in timings)
+    epi_ms = statistics.mean(t["epilogue_ms"] for t in timings)
+    achieved_far = far_pairs * FLOP_FWD / (far_ms * 1e-3)
+    out["forward"] = {
+        "value": poses / (fwd_ms * 1e-3), "unit": "poses/s", "ms_per_field": fwd_ms,
+        "step": "region-list build + near (FP64) + far (FP32x2) kernels + refinement + "
+                "float32 epilogue",
+        "breakdown_ms": {"list_build": list_ms, "near_pairs_fp64": near_ms,
+                         "far_pairs_fp32x2": far_ms, "refine_epilogue": epi_ms},
+        "roofline_far_kernel": {"kernel": "field_far2_kernel<16,8,4,4>", "bound": "fp32",
+                                "achieved": achieved_far / 1e12, "peak": peak / 1e12,
+                                "unit": "TFLOP/s", "frac": achieved_far / peak,
+                                "algorithmic": f"{far_pairs} far in-cutoff pairs x {FLOP_FWD} FLOP",
+                                "traffic": (FAR_DRAM_BYTES_FULL_FIELD
+                                            if args.workload == "full_field" else None)}}
+    del fwd_out
+    # FP64 GPU baselines, one field per launch
+    e64 = torch.empty(shape, dtype=torch.float64, device=device)
+    g64 = torch.empty(shape + (6,), dtype=torch.float64, device=device)
+
+    def plain_adj():
+        system.field_adjoint_device(size, axes, None, None, e64, g64,
+                                    mode=_lib.VEXT_MODE_FP64_PLAIN, stream=stream)
+
+    plain_adj()
+    plain_adj_ms = timed_region(plain_adj, 1, stream)
+    fp64 = {"fp64_plain_fwd_adjoint": {"value": poses / (plain_adj_ms * 1e-3),
+                                       "unit": "poses/s", "ms_per_field": plain_adj_ms}}
+    for label, mode in (("fp64_tiled_forward", _lib.VEXT_MODE_FP64),
+                        ("fp64_plain_forward", _lib.VEXT_MODE_FP64_PLAIN)):
+        times = []
+        for _ in range(2):
+            system.invalidate()
+            torch.cuda.synchronize()
+            system.field(size, axes, mode=mode, orientation=False)
+            st = system.last_stats
+            times.append(st["kernel_ms"] + st["list_build_ms"] + st["epilogue_ms"])
+        fp64[label] = {"value": poses / (min(times) * 1e-3), "unit": "poses/s",
+                       "ms_per_field": min(times)}
+    out["fp64_kernels"] = fp64
+    out["speedup_fwd_adjoint_vs_fp64_plain_fwd_adjoint"] = plain_adj_ms / ms_adj
+    out["speedup_fwd_adjoint_vs_fp64_plain_forward"] = (fp64["fp64_plain_forward"]["ms_per_field"]
+                                                        / ms_adj)
+    out["speedup_forward_vs_fp64_plain_forward"] = (fp64["fp64_plain_forward"]["ms_per_field"]
+                                                    / fwd_ms)
+    # error of the headline result against the plain FP64 forward + adjoint
+    e_mixed64 = torch.empty(shape, dtype=torch.float64, device=device)
+    system.field_adjoint_device(size, axes, energy, grad, e_mixed64, stream=stream)
+    torch.cuda.synchronize()
+    exact = e64.cpu().numpy()
+    err = error_stats(e_mixed64.cpu().numpy(), exact)
+    gx = g64.cpu().numpy()
+    gm = grad.cpu().numpy().astype(np.float64)
+    grel = np.linalg.norm(gm - gx, axis=-1) / np.maximum(np.linalg.norm(gx, axis=-1), 1.0)
+    err["gradient_max_rel"] = float(grel.max())
+    err["gradient_median_rel"] = float(np.median(grel))
+    err["reference"] = "plain FP64 kernel (IEEE division) on the same poses"
+    out["error_vs_fp64"] = err
+    del e64, g64, e_mixed64, exact, gx, gm, grel
+    torch.cuda.empty_cache()
+    system.field(size, axes, orientation=False)
+    out["list_entries"] = system.last_stats["list_entries"]
+    out["near_entries"] = system.last_stats["near_entries"]
+    out["refined_poses_forward"] = system.last_stats["refined_poses"]
+    # forward + adjoint on a random pose batch of the same framework (pose path)
+    n_pose = 1 << 20
+    rng = np.random.default_rng(9)
+    cart = torch.tensor(rng.random((n_pose, 3)) @ case["cell"], device=device)
+    q = torch.tensor(rng.normal(size=(n_pose, 4)), device=device)
+    e = torch.empty(n_pose, dtype=torch.float64, device=device)
+    gc = torch.empty((n_pose, 3), dtype=torch.float64, device=device)
+    gq = torch.empty((n_pose, 4), dtype=torch.float64, device=device)
+
+    def pose_step():
+        system.pose_energy_grad_device(cart, q, e, gc, gq, stream=stream)
+
+    pose_step()
+    pose_ms = timed_region(pose_step, 5, stream) / 5
+    out["pose_fwd_adjoint"] = {"value": n_pose / (pose_ms * 1e-3), "unit": "poses/s",
+                               "poses": n_pose, "workload": "random poses (center, quaternion), "
+                               "same framework", "flop_per_pair": FLOP_FWD_ADJ}
+    del cart, q, e, gc, gq
+    if not args.no_batch:
+        out["batch"] = bench_batch(args, size, axes, device, stream, adjoint=False)
+        out["batch_fwd_adjoint"] = bench_batch(args, size, axes, device, stream, adjoint=True)
+    return out
+
+
+def bench_batch(args, size, axes, device, stream, adjoint=False):
     """The batched workload: 50 seeded frameworks x 2 guests = 100 fields of
-    size^3 x 64 in one persistent, graph-captured launch (autotuned)."""
+    size^3 x 64 in one persistent, graph-captured launch (autotuned);
+    forward only, or forward + adjoint (energy and 6 gradient components)."""
     import torch
     from string_vext_b200 import synth
     from string_vext_b200.system import VextBatch, VextSystem
     t0 = time.perf_counter()
     systems = [VextSystem(c) for c in synth.batch_frameworks()]
-    outs = [torch.empty((len(axes), size, size, size), dtype=torch.float32, device=device)
-            for _ in systems]
-    batch = VextBatch(systems, size, axes, outs)
+    shape = (len(axes), size, size, size)
+    outs = [torch.empty(shape, dtype=torch.float32, device=device) for _ in systems]
+    grads = ([torch.empty(shape + (6,), dtype=torch.float32, device=device) for _ in systems]
+             if adjoint else None)
+    batch = VextBatch(systems, size, axes, outs, gradients=grads)
     setup_s = time.perf_counter() - t0
     info = batch.info()
     for _ in range(max(1, args.warmup // 2)):
@@ -377,13 +473,13 @@ def bench_batch(args, size, axes, device, stream):
     result = {"value": info["poses"] / (ms * 1e-3), "unit": "poses/s", "ms_per_batch": ms,
               "fields": len(systems), "poses": info["poses"], "work_items": info["work_items"],
               "list_gb": info["list_bytes"] / 1e9, "setup_s": setup_s,
-              "autotuned": {"cta_shape": ["128x4 dirs", "256x2 dirs"][info["shape"]],
-                            "resident_ctas": info["grid"]},
-              "workload": "50 seeded frameworks x 2 guests, one graph launch"}
+              "autotuned": {"cta_shape": info["cta_shape"], "resident_ctas": info["grid"]},
+              "workload": "50 seeded frameworks x 2 guests, one graph launch",
+              "step": "forward + adjoint" if adjoint else "forward"}
     batch.close()
     for s_ in systems:
         s_.close()
-    del outs
+    del outs, grads
     torch.cuda.empty_cache()
     return result
 
@@ -396,11 +492,17 @@ def run_profile_case(kind):
     from string_vext_b200.system import VextSystem
     case = synth.full_field()
     with VextSystem(case) as system:
+        _, axes = regular_pose_grid(60, 64)
+        axes = normalized_directors(axes)
         if kind == "field":
-            _, axes = regular_pose_grid(60, 64)
-            axes = normalized_directors(axes)
             for _ in range(2):
                 system.field(60, axes, orientation=False)
+        elif kind == "adjoint":
+            e = torch.empty((64, 60, 60, 60), dtype=torch.float32, device="cuda")
+            g = torch.empty((64, 60, 60, 60, 6), dtype=torch.float32, device="cuda")
+            for _ in range(2):
+                system.field_adjoint_device(60, axes, e, g)
+            torch.cuda.synchronize()
         else:
             n = 1 << 20
             rng = np.random.default_rng(9)
@@ -418,7 +520,7 @@ def run_profile_case(kind):
 def main():
     parser = argparse.ArgumentParser(description=__doc__)
     parser.add_argument("--gpus", type=int, default=1)
-    parser.add_argument("--steps", type=int, default=5)
+    parser.add_argument("--steps", type=int, default=30)
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
     parser.add_argument("--workload", default="full_field",
@@ -427,10 +529,12 @@ def main():
                         help="target length of the CPU-baseline sample")
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     parser.add_argument("--no-batch", action="store_true", help="skip the 100-field batch")
-    parser.add_argument("--profile", choices=("field", "pose"),
+    parser.add_argument("--profile", choices=("field", "adjoint", "pose"),
                         help="run one short case for an ncu capture and exit: 'field' = two "
-                             "mixed full_field fields, 'pose' = two 2^20-pose forward+adjoint "
-                             "batches of the same framework")
+                             "mixed full_field fields (forward), 'adjoint' = two forward + "
+                             "adjoint full_field fields (the first builds, autotunes and "
+                             "captures), 'pose' = two 2^20-pose forward+adjoint batches of the "
+                             "same framework")
     args = parser.parse_args()
     ensure_built()
     if args.profile:

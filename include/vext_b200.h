@@ -294,6 +294,11 @@ VEXT_API int vext_batch_status(vext_batch batch);
 VEXT_API int vext_batch_destroy(vext_batch batch);
 VEXT_API int vext_batch_info(vext_batch batch, int64_t *work_items, int64_t *poses,
                              int64_t *list_bytes, int *shape, int *grid);
+/* The autotuner's candidates (kernel shape index, resident CTAs, sample time
+ * in ms, shape name: threads x directors per thread[/CTAs-per-SM bound]),
+ * at most max_candidates of them; any output may be NULL. */
+VEXT_API int vext_batch_tuning(vext_batch batch, int max_candidates, int *n_candidates,
+                               int *shapes, int *grids, float *ms, const char **names);
 
 /* ------------------------------------------------------------------------ */
 /* Diagnostics. */

@@ -274,7 +274,9 @@ def reference_field_parallel(case, centers_frac, axes, library=REF_KERNEL, proce
                              symbol="evaluate_reused_neighbors"):
     """The reference's multi-process mode (one driver per worker over disjoint
     center shards, as its ``--workers`` batch runners do).  Uses a ``spawn``
-    pool.  Returns (energy (n_centers, n_axes), wall seconds, processes)."""
+    pool.  Returns (energy (n_centers, n_axes), wall seconds including the
+    pool start, processes, compute seconds = the slowest worker's
+    neighbour-query + kernel time)."""
     import multiprocessing as mp
     processes = processes or max(1, len(os.sched_getaffinity(0)))
     shards = np.array_split(np.arange(len(centers_frac)), processes)
@@ -284,4 +286,5 @@ def reference_field_parallel(case, centers_frac, axes, library=REF_KERNEL, proce
     with mp.get_context("spawn").Pool(len(jobs)) as pool:
         parts = pool.map(_shard_worker, jobs)
     wall = time.perf_counter() - t0
-    return np.concatenate([p[0] for p in parts]), wall, len(jobs)
+    return (np.concatenate([p[0] for p in parts]), wall, len(jobs),
+            max(p[1] for p in parts))

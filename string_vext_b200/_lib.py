@@ -132,6 +132,10 @@ def load() -> ctypes.CDLL:
     lib.vext_field_adjoint_device.restype = ci
     lib.vext_field_adjoint.argtypes = [vp, ci, ci, vp, ctypes.POINTER(Options), vp, vp]
     lib.vext_field_adjoint.restype = ci
+    lib.vext_batch_tuning.argtypes = [vp, ci, ctypes.POINTER(ci), ctypes.POINTER(ci),
+                                      ctypes.POINTER(ci), ctypes.POINTER(ctypes.c_float),
+                                      ctypes.POINTER(ctypes.c_char_p)]
+    lib.vext_batch_tuning.restype = ci
     lib.vext_batch_run.argtypes = [vp, vp]
     lib.vext_batch_run.restype = ci
     lib.vext_batch_status.argtypes = [vp]

@@ -60,7 +60,9 @@ struct BatchArgs {
 
 // Forward + adjoint item: the same staged pipeline with the AdjAcc pair loops
 // (pair.cuh); writes the energy and [dE/dc, tangent dE/du] of every pose.
-template <int CB, int G, int P>
+// Far entries come in two passes: inner (no cutoff mask, shift summed once
+// per entry) and shell.
+template <int CB, int G, int P, bool NEWTON, bool RCP1>
 __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSys &y,
                                                const RegionInfo &r, Stager &st, double *ed,
                                                const float4 *stf, const double *std4,
@@ -96,6 +98,7 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
         }
         seq += plan.n_chunks;
     }
+    double shift_sum = 0.0;
     {
         float2 ux[PP], uy[PP], uz[PP];
 #pragma unroll
@@ -107,30 +110,42 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
             uz[j] = make_float2((float)y.axes[3 * o0 + 2], (float)y.axes[3 * o1 + 2]);
         }
         const FarGeom g = far_geom(cx, cy, cz, y.off0, y.off1, y.rc2f);
-        ChunkPlan plan;
-        plan.init_range(r.off + r.n_near, 0, r.n_total - r.n_near);
-        stage_prologue(st, plan, y.hi, y.lo, seq);
-        for (int c = 0; c < plan.n_chunks; ++c) {
-            if (!stage_wait(st, plan, c, seq, a.status)) return false;
-            int start, len;
-            bool near;
-            plan.chunk(c, start, len, near);
-            far_chunk_adj<P, true, 16>(st.hib + ((seq + c) % kStages) * kCH, stf, len, g, ux, uy,
-                                       uz, acc);
-            stage_next(st, plan, y.hi, y.lo, c, seq);
+#pragma unroll 1
+        for (int pass = 0; pass < 2; ++pass) {   // inner entries, then the shell
+            ChunkPlan plan;
+            plan.init_range(r.off + r.n_near + (pass ? r.n_inner : 0), 0,
+                            pass ? r.n_total - r.n_near - r.n_inner : r.n_inner);
+            stage_prologue(st, plan, y.hi, y.lo, seq);
+            for (int c = 0; c < plan.n_chunks; ++c) {
+                if (!stage_wait(st, plan, c, seq, a.status)) return false;
+                int start, len;
+                bool near;
+                plan.chunk(c, start, len, near);
+                const float4 *hb = st.hib + ((seq + c) % kStages) * kCH;
+                if (pass)
+                    far_chunk_adj<P, NEWTON, 16, true, RCP1>(hb, stf, len, g, ux, uy, uz, acc,
+                                                             shift_sum);
+                else
+                    far_chunk_adj<P, NEWTON, 16, false, RCP1>(hb, stf, len, g, ux, uy, uz, acc,
+                                                              shift_sum);
+                stage_next(st, plan, y.hi, y.lo, c, seq);
+            }
+            seq += plan.n_chunks;
         }
-        seq += plan.n_chunks;
     }
 #pragma unroll
     for (int p = 0; p < P; ++p) {
         const int o = min(obase + G * p, y.O - 1);
+        acc[p].e += 2.0 * shift_sum;
         adj_finish(acc[p], y.off0, y.off1, y.axes[3 * o], y.axes[3 * o + 1], y.axes[3 * o + 2],
                    e[p], gr[p]);
     }
     return true;
 }
 
-template <int CB, int G, int P, int MINB, bool ADJ>
+// ADJ: 0 = forward; forward + adjoint with the far reciprocal taken as
+// 1 = rcp(q) cubed (default), 2 = rcp(q^3) + Newton, 3 = rcp(q^3).
+template <int CB, int G, int P, int MINB, int ADJ>
 __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
     constexpr int NT = CB * G, PP = P / 2;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -171,8 +186,8 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
         double e[P];
         double gr[ADJ ? P : 1][6];
         if constexpr (ADJ) {
-            if (!batch_item_adj<CB, G, P>(a, y, r, st, ed, stf, std4, seq, cx, cy, cz, obase, e,
-                                          gr))
+            if (!batch_item_adj<CB, G, P, ADJ == 2, ADJ == 1>(a, y, r, st, ed, stf, std4, seq,
+                                                              cx, cy, cz, obase, e, gr))
                 return;
         } else {
         // ---- near pairs (FP64)
@@ -220,21 +235,27 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
                 acc[2 * j] = acc[2 * j + 1] = 0.0;
             }
             const FarGeom g = far_geom(cx, cy, cz, y.off0, y.off1, y.rc2f);
-            ChunkPlan plan;
-            plan.init_range(r.off + r.n_near, 0, r.n_total - r.n_near);
-            stage_prologue(st, plan, y.hi, y.lo, seq);
-            for (int c = 0; c < plan.n_chunks; ++c) {
-                if (!stage_wait(st, plan, c, seq, a.status)) return;
-                int start, len;
-                bool near;
-                plan.chunk(c, start, len, near);
-                far_chunk<P, true, 16, false, true>(st.hib + ((seq + c) % kStages) * kCH, stf,
-                                                    len, g, ux, uy, uz, acc);
-                stage_next(st, plan, y.hi, y.lo, c, seq);
+            double shift_sum = 0.0;
+#pragma unroll 1
+            for (int pass = 0; pass < 2; ++pass) {   // inner entries, then the shell
+                ChunkPlan plan;
+                plan.init_range(r.off + r.n_near + (pass ? r.n_inner : 0), 0,
+                                pass ? r.n_total - r.n_near - r.n_inner : r.n_inner);
+                stage_prologue(st, plan, y.hi, y.lo, seq);
+                for (int c = 0; c < plan.n_chunks; ++c) {
+                    if (!stage_wait(st, plan, c, seq, a.status)) return;
+                    int start, len;
+                    bool near;
+                    plan.chunk(c, start, len, near);
+                    const float4 *hb = st.hib + ((seq + c) % kStages) * kCH;
+                    if (pass) far_chunk_fwd<P, 16, true>(hb, stf, len, g, ux, uy, uz, acc, shift_sum);
+                    else far_chunk_fwd<P, 16, false>(hb, stf, len, g, ux, uy, uz, acc, shift_sum);
+                    stage_next(st, plan, y.hi, y.lo, c, seq);
+                }
+                seq += plan.n_chunks;
             }
-            seq += plan.n_chunks;
 #pragma unroll
-            for (int p = 0; p < P; ++p) e[p] += acc[p];
+            for (int p = 0; p < P; ++p) e[p] += acc[p] + 2.0 * shift_sum;
         }
         }
         if (cvalid) {
@@ -320,29 +341,55 @@ __global__ void batch_refine_kernel(BatchArgs a) {
 // ---------------------------------------------------------------- host side
 
 struct BatchConfig {
-    int shape;   // index into the mode's kernel table (batch_kernels)
+    int shape;   // index into the mode's kernel table (batch_kernel)
     int grid;    // resident CTAs (persistent grid)
 };
 
 // CTA shapes the autotuner chooses from; every shape covers a 32-director
 // block (G x P = 32).  Forward: <16, 8, 4> x 128 threads or <16, 16, 2> x 256.
-// Forward + adjoint (9 FP64 sums per director): <16, 16, 2> x 256 or
-// <16, 8, 4> x 128 with fewer CTAs per SM.
+// Forward + adjoint (9 FP64 sums per director): <16, 16, 2> x 256, or
+// <16, 8, 4> x 128 bounded to 2 or 3 CTAs per SM (225 / 168 registers).
 struct BatchKernel {
     void (*fn)(BatchArgs);
     int threads;
     const char *name;
 };
 
-static const BatchKernel kForwardKernels[2] = {
-    {batch_field_kernel<16, 8, 4, 4, false>, 128, "128x4"},
-    {batch_field_kernel<16, 16, 2, 3, false>, 256, "256x2"}};
-static const BatchKernel kAdjointKernels[2] = {
-    {batch_field_kernel<16, 16, 2, 2, true>, 256, "256x2"},
-    {batch_field_kernel<16, 8, 4, 2, true>, 128, "128x4"}};
+static const BatchKernel kForwardKernels[] = {
+    {batch_field_kernel<16, 8, 4, 4, 0>, 128, "128x4"},
+    {batch_field_kernel<16, 16, 2, 3, 0>, 256, "256x2"}};
+static const BatchKernel kAdjointKernels[] = {
+    {batch_field_kernel<16, 16, 2, 2, 1>, 256, "256x2"},
+    {batch_field_kernel<16, 8, 4, 2, 1>, 128, "128x4"},
+    {batch_field_kernel<16, 8, 4, 3, 1>, 128, "128x4/3"}};
+static const BatchKernel kAdjointNewtonKernels[] = {   // accuracy/speed study
+    {batch_field_kernel<16, 16, 2, 2, 2>, 256, "256x2 rcp3+newton"},
+    {batch_field_kernel<16, 8, 4, 2, 2>, 128, "128x4 rcp3+newton"}};
+static const BatchKernel kAdjointRcp3Kernels[] = {     // accuracy/speed study
+    {batch_field_kernel<16, 16, 2, 2, 3>, 256, "256x2 rcp3"},
+    {batch_field_kernel<16, 8, 4, 2, 3>, 128, "128x4 rcp3"}};
+constexpr int kMaxCandidates = 8;
 
-static const BatchKernel &batch_kernel(bool adj, int shape) {
-    return adj ? kAdjointKernels[shape] : kForwardKernels[shape];
+#define VEXT_COUNT(t) (int)(sizeof t / sizeof t[0])
+
+// kind: 0 forward, 1 forward + adjoint (default: reciprocal of q, cubed),
+// 2 with the reciprocal of q^3 and a Newton step, 3 the same without it
+static int batch_kernel_count(int kind) {
+    switch (kind) {
+    case 0: return VEXT_COUNT(kForwardKernels);
+    case 1: return VEXT_COUNT(kAdjointKernels);
+    case 2: return VEXT_COUNT(kAdjointNewtonKernels);
+    default: return VEXT_COUNT(kAdjointRcp3Kernels);
+    }
+}
+
+static const BatchKernel &batch_kernel(int kind, int shape) {
+    switch (kind) {
+    case 0: return kForwardKernels[shape];
+    case 1: return kAdjointKernels[shape];
+    case 2: return kAdjointNewtonKernels[shape];
+    default: return kAdjointRcp3Kernels[shape];
+    }
 }
 
 }  // namespace vext
@@ -364,7 +411,10 @@ struct vext_batch_s {
     int64_t poses = 0, list_bytes = 0;
     BatchConfig config{0, 0};
     bool adj = false;
-    float tune_ms[4] = {0, 0, 0, 0};
+    int kind = 0;   // batch_kernel table
+    BatchConfig cands[kMaxCandidates] = {};
+    int n_cands = 0;
+    float tune_ms[kMaxCandidates] = {};
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -401,7 +451,7 @@ static int batch_launch(vext_batch b, const BatchConfig &cfg, const int4 *items,
     const size_t smem = batch_smem(b->max_types);
     VEXT_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(int), st));
     VEXT_CUDA(cudaMemsetAsync(b->d_refine, 0, sizeof(int), st));
-    const BatchKernel &k = batch_kernel(b->adj, cfg.shape);
+    const BatchKernel &k = batch_kernel(b->kind, cfg.shape);
     k.fn<<<cfg.grid, k.threads, smem, st>>>(a);
     VEXT_CUDA(cudaGetLastError());
     if (b->opt.band_hi > b->opt.band_lo) {
@@ -438,6 +488,7 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
     b->n_axes = n_axes;
     b->opt = resolve_options(opt);
     b->adj = gradients != nullptr;
+    b->kind = !b->adj ? 0 : (b->opt.variant & 32) ? 2 : (b->opt.variant & 64) ? 3 : 1;
     if (b->opt.mode != VEXT_MODE_MIXED)
         return fail(VEXT_ERR_ARGUMENT, "batched fields run in the mixed mode only");
     int dev = 0;
@@ -513,23 +564,28 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
     VEXT_CUDA(cudaMemset(b->d_status, 0, sizeof(int)));
     // ---- autotune: CTA shape x resident CTAs per SM, on the sampled queue
     const size_t smem = batch_smem(b->max_types);
-    int sms = 0, occ[2] = {0, 0};
+    int sms = 0;
     VEXT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    for (int k = 0; k < 2; ++k) {
-        const BatchKernel &bk = batch_kernel(b->adj, k);
+    // candidates: every kernel of the mode at its full and at half its occupancy
+    BatchConfig cands[kMaxCandidates];
+    int n_cands = 0;
+    for (int k = 0; k < batch_kernel_count(b->kind); ++k) {
+        const BatchKernel &bk = batch_kernel(b->kind, k);
         VEXT_CUDA(cudaFuncSetAttribute(bk.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
-        VEXT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[k], bk.fn, bk.threads, smem));
+        int occ = 0;
+        VEXT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bk.fn, bk.threads, smem));
+        if (occ < 1) continue;
+        cands[n_cands++] = {k, sms * occ};
+        if (occ >= 2 && n_cands < kMaxCandidates) cands[n_cands++] = {k, sms * (occ / 2)};
     }
-    const int occ0 = occ[0], occ1 = occ[1];
-    if (occ0 < 1 || occ1 < 1) return fail(VEXT_ERR_CAPACITY, "batch kernel does not fit an SM");
-    const BatchConfig cands[4] = {{0, sms * occ0}, {0, sms * std::max(1, occ0 / 2)},
-                                  {1, sms * occ1}, {1, sms * std::max(1, occ1 / 2)}};
+    if (n_cands == 0) return fail(VEXT_ERR_CAPACITY, "batch kernel does not fit an SM");
+    b->n_cands = n_cands;
     cudaEvent_t e0, e1;
     VEXT_CUDA(cudaEventCreate(&e0));
     VEXT_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
-    for (int c = 0; c < 4; ++c) {
+    for (int c = 0; c < n_cands; ++c) {
         VEXT_TRY(batch_launch(b, cands[c], b->d_sample, b->n_sample, b->stream));   // warm-up
         VEXT_CUDA(cudaEventRecord(e0, b->stream));
         VEXT_TRY(batch_launch(b, cands[c], b->d_sample, b->n_sample, b->stream));
@@ -538,6 +594,7 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
         float ms = 0;
         VEXT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
         b->tune_ms[c] = ms;
+        b->cands[c] = cands[c];
         if (ms < best) {
             best = ms;
             b->config = cands[c];
@@ -612,6 +669,19 @@ extern "C" int vext_batch_status(vext_batch b) {
 
 extern "C" int vext_batch_destroy(vext_batch b) {
     delete b;
+    return 0;
+}
+
+extern "C" int vext_batch_tuning(vext_batch b, int max_candidates, int *n_candidates,
+                                 int *shapes, int *grids, float *ms, const char **names) {
+    if (!b) return fail(VEXT_ERR_ARGUMENT, "null batch");
+    if (n_candidates) *n_candidates = b->n_cands;
+    for (int c = 0; c < std::min(max_candidates, b->n_cands); ++c) {
+        if (shapes) shapes[c] = b->cands[c].shape;
+        if (grids) grids[c] = b->cands[c].grid;
+        if (ms) ms[c] = b->tune_ms[c];
+        if (names) names[c] = batch_kernel(b->kind, b->cands[c].shape).name;
+    }
     return 0;
 }
 

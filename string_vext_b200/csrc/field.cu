@@ -183,6 +183,78 @@ __global__ void __launch_bounds__(CB *G, MINB) field_far_kernel(FieldArgs a) {
     }
 }
 
+// The default far kernel: far_chunk_fwd over the inner entries (no mask) and
+// then the shell entries; same thread layout and output as field_far_kernel.
+template <int CB, int G, int P, int MINB>
+__global__ void __launch_bounds__(CB *G, MINB) field_far2_kernel(FieldArgs a) {
+    constexpr int NT = CB * G, PP = P / 2;
+    extern __shared__ __align__(128) unsigned char smem[];
+    Stager st;
+    st.bar = reinterpret_cast<uint64_t *>(smem);
+    st.hib = reinterpret_cast<float4 *>(smem + 64);
+    st.lob = st.hib;   // far chunks bring hi only
+    float4 *stf = st.hib + kStages * kCH;
+
+    const int tid = threadIdx.x;
+    const RegionInfo r = a.regs[blockIdx.x];
+    load_types<NT>(stf, nullptr, a.tf, a.td, a.n_types);
+    init_barriers(st);
+    __syncthreads();
+
+    const int cl = tid % CB, og = tid / CB;
+    const bool cvalid = cl < r.ni * r.nj * r.nk;
+    int gi, gj, gk;
+    center_of(a, r, cvalid ? cl : 0, gi, gj, gk);
+    double cxd, cyd, czd;
+    frac_to_cart(a.H, (gi + .5) / a.S - r.of[0], (gj + .5) / a.S - r.of[1],
+                 (gk + .5) / a.S - r.of[2], cxd, cyd, czd);
+    const FarGeom g = far_geom(cxd, cyd, czd, a.off0, a.off1, a.rc2f);
+    const int obase = blockIdx.y * (G * P) + og;
+    float2 ux[PP], uy[PP], uz[PP];
+    double acc[P];
+#pragma unroll
+    for (int j = 0; j < PP; ++j) {
+        const int o0 = min(obase + G * (2 * j), a.O - 1), o1 = min(obase + G * (2 * j + 1), a.O - 1);
+        ux[j] = make_float2((float)a.axes[3 * o0], (float)a.axes[3 * o1]);
+        uy[j] = make_float2((float)a.axes[3 * o0 + 1], (float)a.axes[3 * o1 + 1]);
+        uz[j] = make_float2((float)a.axes[3 * o0 + 2], (float)a.axes[3 * o1 + 2]);
+        acc[2 * j] = acc[2 * j + 1] = 0.0;
+    }
+    double shift_sum = 0.0;
+    unsigned seq = 0;
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {   // inner entries, then the shell
+        ChunkPlan plan;
+        plan.init_range(r.off + r.n_near + (pass ? r.n_inner : 0), 0,
+                        pass ? r.n_total - r.n_near - r.n_inner : r.n_inner);
+        stage_prologue(st, plan, a.hi, a.lo, seq);
+        for (int c = 0; c < plan.n_chunks; ++c) {
+            if (!stage_wait(st, plan, c, seq, a.status)) return;
+            int start, len;
+            bool near;
+            plan.chunk(c, start, len, near);
+            const float4 *hb = st.hib + ((seq + c) % kStages) * kCH;
+            if (pass) far_chunk_fwd<P, 16, true>(hb, stf, len, g, ux, uy, uz, acc, shift_sum);
+            else far_chunk_fwd<P, 16, false>(hb, stf, len, g, ux, uy, uz, acc, shift_sum);
+            stage_next(st, plan, a.hi, a.lo, c, seq);
+        }
+        seq += plan.n_chunks;
+    }
+    if (cvalid) {
+        const size_t S3 = (size_t)a.S * a.S * a.S;
+        const size_t cg = ((size_t)gi * a.S + gj) * a.S + gk;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            const int o = obase + G * p;
+            if (o < a.O) {
+                double *dst = a.e64b ? a.e64b : a.e64;   // separate buffer when run concurrently
+                dst[(size_t)o * S3 + cg] =
+                    (a.e64b ? 0.0 : dst[(size_t)o * S3 + cg]) + acc[p] + 2.0 * shift_sum;
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------- epilogue
 
 __global__ void flag_kernel(const double *e64, long long n, double lo, double hi, int *list) {
@@ -500,7 +572,9 @@ static int launch_near(const FieldArgs &a, int cb, int mode, cudaStream_t stream
 }
 
 // Far-kernel variants (threads = CB x G, directors per CTA = G x P):
-//   0 (default): <16, 8, 4>, 4 CTAs/SM of 128, one reciprocal of q^3 per lane
+//   0 (default): field_far2_kernel <16, 8, 4>, 4 CTAs/SM of 128: inner entries
+//      without the cutoff mask, reciprocal of q per lane cubed, no Newton step
+//   9: field_far_kernel <16, 8, 4>: reciprocal of q^3 per lane + Newton step
 //   5: the same with one reciprocal per two lanes (1/(qx qy)) and cubing
 //   1: <16, 16, 4>, 2 CTAs/SM    2: <16, 32, 2>, 1 CTA of 512/SM
 //   3: <16, 16, 2>, 3 CTAs/SM    4: <16, 16, 4>, 3 CTAs/SM
@@ -525,9 +599,10 @@ static int launch_far(const FieldArgs &a, int cb, int variant, cudaStream_t stre
     case 4: return launch_t(field_far_kernel<16, 16, 4, 3>, grid_for(64), 256, smem, a, stream);
     case 1: return launch_t(field_far_kernel<16, 16, 4, 2>, grid_for(64), 256, smem, a, stream);
     case 5: return launch_t(field_far_kernel<16, 8, 4, 4>, grid_for(32), 128, smem, a, stream);
-    default:
+    case 9:
         return launch_t(field_far_kernel<16, 8, 4, 4, true, 16, false, true>, grid_for(32), 128,
                         smem, a, stream);
+    default: return launch_t(field_far2_kernel<16, 8, 4, 4>, grid_for(32), 128, smem, a, stream);
     }
 }
 
@@ -762,7 +837,8 @@ static int field_adjoint_device(vext_system h, int size, int n_axes, const doubl
                           sys->adj_axes.size() == 3 * (size_t)n_axes &&
                           std::equal(axes, axes + 3 * n_axes, sys->adj_axes.begin()) &&
                           sys->adj_key[0] == o.r_split && sys->adj_key[1] == o.band_lo &&
-                          sys->adj_key[2] == o.band_hi && sys->adj_energy == energy &&
+                          sys->adj_key[2] == o.band_hi && sys->adj_key[3] == o.variant &&
+                          sys->adj_energy == energy &&
                           sys->adj_grad == gradient && sys->adj_energy64 == energy_f64;
         if (!same) {
             sys->drop_adjoint_batch();
@@ -775,6 +851,7 @@ static int field_adjoint_device(vext_system h, int size, int n_axes, const doubl
             sys->adj_key[0] = o.r_split;
             sys->adj_key[1] = o.band_lo;
             sys->adj_key[2] = o.band_hi;
+            sys->adj_key[3] = o.variant;
             sys->adj_energy = energy;
             sys->adj_grad = gradient;
             sys->adj_energy64 = energy_f64;

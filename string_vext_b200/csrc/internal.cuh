@@ -34,7 +34,9 @@ struct alignas(16) RegionInfo {
     int n_total;        // all entries
     int i0, j0, k0;     // first grid center (field regions)
     int ni, nj, nk;     // grid centers per axis (field regions)
-    int pad[2];
+    int n_inner;        // far entries within the cutoff of every site of every pose of the
+                        // region (they follow the near entries; the shell ones come last)
+    int pad;
 };
 static_assert(sizeof(RegionInfo) % 16 == 0, "RegionInfo must stay 16-byte aligned");
 
@@ -104,7 +106,7 @@ struct System {
     vext_batch adj_batch = nullptr;
     int adj_size = 0;
     std::vector<double> adj_axes;
-    double adj_key[3] = {0, 0, 0};   // r_split, band_lo, band_hi
+    double adj_key[4] = {0, 0, 0, 0};   // r_split, band_lo, band_hi, variant
     float *adj_energy = nullptr, *adj_grad = nullptr;
     double *adj_energy64 = nullptr;
     float *d_g32 = nullptr;          // host-output staging of the float32 gradient

@@ -16,14 +16,17 @@ __device__ __forceinline__ float set_lt(float a, float b) {
     return r;
 }
 
-// FP64 reciprocal: hardware seed refined by two Newton-Raphson steps
-// r' = r + r (1 - s r).  Each step squares the relative error; one step
-// leaves a measurable one-sided (under-estimating) bias, two do not.
+// FP64 reciprocal: hardware seed (relative error <= 2^-23) refined by
+// Newton-Raphson steps r' = r + r (1 - s r), each squaring the relative error
+// and leaving it one-sided (r under-estimates): one step leaves <= 2^-46
+// (1.4e-14, far below the mixed-precision bar), two reach FP64 rounding.
+template <int STEPS = 2>
 __device__ __forceinline__ double rcp64_nr(double s) {
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(s));
-    r = fma(r, fma(-s, r, 1.0), r);
-    return fma(r, fma(-s, r, 1.0), r);
+#pragma unroll
+    for (int k = 0; k < STEPS; ++k) r = fma(r, fma(-s, r, 1.0), r);
+    return r;
 }
 
 // ------------------------------------------------------------ staging
@@ -119,8 +122,8 @@ __device__ __forceinline__ NearGeom near_geom(double cx, double cy, double cz, d
 //          cutoff test.
 //   MODE 1/2 (mixed): the thread's poses share one grid center c, so with
 //          d0 = x - c, t = d0 . u:  q_s = |d0|^2 + o_s^2 - 2 o_s t (|d0|^2
-//          once per entry, 1 FMA per site after t); Newton-refined
-//          reciprocal.  MODE 2 drops the cutoff test (near pairs are never
+//          once per entry, 1 FMA per site after t); reciprocal refined
+//          by one Newton step.  MODE 2 drops the cutoff test (near pairs are never
 //          farther apart than r_split + 2 rho_site < rc, checked on the host).
 template <int P, int MODE>
 __device__ __forceinline__ void near_chunk(const double *ed, const double *std4, int len,
@@ -160,7 +163,7 @@ __device__ __forceinline__ void near_chunk(const double *ed, const double *std4,
                 for (int q = 0; q < 2; ++q) {
                     const double d2 = fma(q ? g.m1 : g.m0, tt, q ? k1 : k0);
                     const double s2 = fmax(d2, sh.y);
-                    const double i2 = rcp64_nr(s2);
+                    const double i2 = rcp64_nr<1>(s2);
                     const double i6 = i2 * i2 * i2;
                     const double en = fma(i6, fma(cc.x, i6, -cc.y), sh.x);
                     if (MODE == 1) acc[p][q] += d2 < g.rc2 ? en : 0.0;
@@ -272,6 +275,68 @@ __device__ __forceinline__ void far_chunk(const float4 *hb, const float4 *stf, i
     }
 }
 
+// Forward far chunk, the default: per lane n1 = hardware reciprocal of q (no
+// Newton step), n3 = n1^3 = q^-3, e = n3 (c12 n3 - c6); MASK as in
+// far_chunk_adj (inner entries: no mask, shift summed once per entry into
+// shift_sum, to be added twice -- both sites -- to every energy).  FP32
+// partials over FLUSH entries are flushed into the FP64 acc.
+template <int P, int FLUSH, bool MASK>
+__device__ __forceinline__ void far_chunk_fwd(const float4 *hb, const float4 *stf, int len,
+                                              const FarGeom &g, const float2 (&ux)[P / 2],
+                                              const float2 (&uy)[P / 2],
+                                              const float2 (&uz)[P / 2], double (&acc)[P],
+                                              double &shift_sum) {
+    constexpr int PP = P / 2;
+#pragma unroll 1
+    for (int e0 = 0; e0 < len; e0 += FLUSH) {
+        float2 fa[PP];
+        float fs = 0.f;
+#pragma unroll
+        for (int j = 0; j < PP; ++j) fa[j] = make_float2(0.f, 0.f);
+        const int e1 = min(e0 + FLUSH, len);
+#pragma unroll 2
+        for (int e = e0; e < e1; ++e) {
+            const float4 h = hb[e];
+            const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, -)
+            const float dx = h.x - g.cx, dy = h.y - g.cy, dz = h.z - g.cz;
+            const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float2 k0 = make_float2(dd + g.oo0, dd + g.oo0),
+                         k1 = make_float2(dd + g.oo1, dd + g.oo1);
+            const float2 dx2 = make_float2(dx, dx), dy2 = make_float2(dy, dy),
+                         dz2 = make_float2(dz, dz);
+            const float2 c12 = make_float2(tp.x, tp.x), mc6 = make_float2(-tp.y, -tp.y),
+                         sh = make_float2(tp.z, tp.z);
+            if (!MASK) fs += tp.z;
+#pragma unroll
+            for (int j = 0; j < PP; ++j) {
+                const float2 t =
+                    __ffma2_rn(dx2, ux[j], __ffma2_rn(dy2, uy[j], __fmul2_rn(dz2, uz[j])));
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const float2 d2 = __ffma2_rn(q ? g.m1 : g.m0, t, q ? k1 : k0);
+                    float r0, r1;
+                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(d2.x));
+                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r1) : "f"(d2.y));
+                    const float2 n1 = make_float2(r0, r1);
+                    float2 n3 = __fmul2_rn(__fmul2_rn(n1, n1), n1);
+                    if (MASK) {
+                        const float2 m = make_float2(set_lt(d2.x, g.rc2f), set_lt(d2.y, g.rc2f));
+                        n3 = __fmul2_rn(n3, m);
+                        fa[j] = __ffma2_rn(m, sh, fa[j]);
+                    }
+                    fa[j] = __ffma2_rn(n3, __ffma2_rn(c12, n3, mc6), fa[j]);
+                }
+            }
+        }
+        if (!MASK) shift_sum += (double)fs;
+#pragma unroll
+        for (int j = 0; j < PP; ++j) {
+            acc[2 * j] += (double)fa[j].x;
+            acc[2 * j + 1] += (double)fa[j].y;
+        }
+    }
+}
+
 // ------------------------------------------------------------ adjoint
 //
 // Forward + adjoint sums of one pose (center c, unit director u, sites at
@@ -345,7 +410,7 @@ __device__ __forceinline__ void near_chunk_adj(const double *ed, const double *s
             for (int q = 0; q < 2; ++q) {
                 const double d2 = fma(q ? g.m1 : g.m0, tt, q ? k1 : k0);
                 const double s2 = fmax(d2, sh.y);
-                const double i2 = rcp64_nr(s2);
+                const double i2 = rcp64_nr<1>(s2);
                 const double i6 = i2 * i2 * i2;
                 double en = fma(i6, fma(cc.x, i6, -cc.y), sh.x);
                 double fp = d2 < sh.y ? 0.0 : (i6 * i2) * fma(m2c12, i6, cc.y);
@@ -365,20 +430,28 @@ __device__ __forceinline__ void near_chunk_adj(const double *ed, const double *s
 }
 
 // Packed FP32x2 far chunk, forward + adjoint (lanes = two directors).  Per
-// site: n3 = -1/q^3 (hardware reciprocal of -q^3, NEWTON-refined), m = 1/0
-// cutoff mask, n3m = n3 m;  e = n3m (c12 n3m + c6) + m shift;  fp = n3m (2 c12
-// n3m + c6) (n3 q^2) = (dE/dq) / 3.  FP32 partials over FLUSH entries are
-// flushed into the FP64 AdjAcc.
-template <int P, bool NEWTON, int FLUSH>
+// site, by default (RCP1): n1 = hardware reciprocal of q per lane, n3 = n1^3 =
+// q^-3, e = n3 (c12 n3 - c6) + m shift, fp = (n1 n3) (c6 - 2 c12 n3) =
+// (dE/dq) / 3, with m the 1/0 cutoff mask folded into n3.  The alternative
+// (RCP1 = false): n3 = reciprocal of -q^3, e = n3 (c12 n3 + c6), fp = n3 (2 c12
+// n3 + c6) (n3 q^2).  NEWTON refines the reciprocal by one Newton step.
+// MASK = false for inner entries (inside the cutoff of every site of every
+// pose of the region): no mask, and the shift, the same for every pose, is
+// summed once per entry into shift_sum (the caller adds 2 x shift_sum, both
+// sites, to every energy).  FP32 partials over FLUSH entries are flushed into
+// the FP64 AdjAcc.
+template <int P, bool NEWTON, int FLUSH, bool MASK, bool RCP1 = true>
 __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *stf, int len,
                                               const FarGeom &g, const float2 (&ux)[P / 2],
                                               const float2 (&uy)[P / 2],
-                                              const float2 (&uz)[P / 2], AdjAcc (&acc)[P]) {
+                                              const float2 (&uz)[P / 2], AdjAcc (&acc)[P],
+                                              double &shift_sum) {
     constexpr int PP = P / 2;
     const float2 one2 = make_float2(1.f, 1.f);
 #pragma unroll 1
     for (int e0 = 0; e0 < len; e0 += FLUSH) {
         float2 fe[PP], fh[PP][2][3], ff[PP][2];
+        float fs = 0.f;
 #pragma unroll
         for (int j = 0; j < PP; ++j) {
             fe[j] = make_float2(0.f, 0.f);
@@ -401,8 +474,8 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
             const float2 dx2 = make_float2(dx, dx), dy2 = make_float2(dy, dy),
                          dz2 = make_float2(dz, dz);
             const float2 c12 = make_float2(tp.x, tp.x), c6 = make_float2(tp.y, tp.y),
-                         sh = make_float2(tp.z, tp.z),
-                         c12x2 = make_float2(2.f * tp.x, 2.f * tp.x);
+                         sh = make_float2(tp.z, tp.z);
+            if (!MASK) fs += tp.z;
 #pragma unroll
             for (int j = 0; j < PP; ++j) {
                 const float2 t =
@@ -410,19 +483,46 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
                     const float2 d2 = __ffma2_rn(q ? g.m1 : g.m0, t, q ? k1 : k0);
-                    const float2 dsq = __fmul2_rn(d2, d2);
-                    const float2 d6 = __fmul2_rn(dsq, d2);
-                    float r0, r1;
-                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(-d6.x));
-                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r1) : "f"(-d6.y));
-                    float2 n3 = make_float2(r0, r1);
-                    if (NEWTON) n3 = __ffma2_rn(n3, __ffma2_rn(d6, n3, one2), n3);
-                    const float2 m = make_float2(set_lt(d2.x, g.rc2f), set_lt(d2.y, g.rc2f));
-                    const float2 n3m = __fmul2_rn(n3, m);
-                    fe[j] = __ffma2_rn(n3m, __ffma2_rn(c12, n3m, c6), fe[j]);
-                    fe[j] = __ffma2_rn(m, sh, fe[j]);
-                    const float2 ea = __fmul2_rn(n3m, __ffma2_rn(c12x2, n3m, c6));
-                    const float2 fp = __fmul2_rn(ea, __fmul2_rn(n3, dsq));
+                    float2 fp;
+                    if (RCP1) {
+                        const float2 mc6 = make_float2(-tp.y, -tp.y),
+                                     m2c12 = make_float2(-2.f * tp.x, -2.f * tp.x);
+                        float r0, r1;
+                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(d2.x));
+                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r1) : "f"(d2.y));
+                        float2 n1 = make_float2(r0, r1);
+                        if (NEWTON)
+                            n1 = __ffma2_rn(n1, __ffma2_rn(make_float2(-d2.x, -d2.y), n1, one2),
+                                            n1);
+                        float2 n3 = __fmul2_rn(__fmul2_rn(n1, n1), n1);
+                        if (MASK) {
+                            const float2 m =
+                                make_float2(set_lt(d2.x, g.rc2f), set_lt(d2.y, g.rc2f));
+                            n3 = __fmul2_rn(n3, m);
+                            fe[j] = __ffma2_rn(m, sh, fe[j]);
+                        }
+                        fe[j] = __ffma2_rn(n3, __ffma2_rn(c12, n3, mc6), fe[j]);
+                        fp = __fmul2_rn(__fmul2_rn(n1, n3), __ffma2_rn(m2c12, n3, c6));
+                    } else {
+                        const float2 c12x2 = make_float2(2.f * tp.x, 2.f * tp.x);
+                        const float2 dsq = __fmul2_rn(d2, d2);
+                        const float2 d6 = __fmul2_rn(dsq, d2);
+                        float r0, r1;
+                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(-d6.x));
+                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r1) : "f"(-d6.y));
+                        float2 n3 = make_float2(r0, r1);
+                        if (NEWTON) n3 = __ffma2_rn(n3, __ffma2_rn(d6, n3, one2), n3);
+                        float2 n3m = n3;
+                        if (MASK) {
+                            const float2 m =
+                                make_float2(set_lt(d2.x, g.rc2f), set_lt(d2.y, g.rc2f));
+                            n3m = __fmul2_rn(n3, m);
+                            fe[j] = __ffma2_rn(m, sh, fe[j]);
+                        }
+                        fe[j] = __ffma2_rn(n3m, __ffma2_rn(c12, n3m, c6), fe[j]);
+                        const float2 ea = __fmul2_rn(n3m, __ffma2_rn(c12x2, n3m, c6));
+                        fp = __fmul2_rn(ea, __fmul2_rn(n3, dsq));
+                    }
                     fh[j][q][0] = __ffma2_rn(fp, dx2, fh[j][q][0]);
                     fh[j][q][1] = __ffma2_rn(fp, dy2, fh[j][q][1]);
                     fh[j][q][2] = __ffma2_rn(fp, dz2, fh[j][q][2]);
@@ -430,6 +530,7 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
                 }
             }
         }
+        if (!MASK) shift_sum += (double)fs;
 #pragma unroll
         for (int j = 0; j < PP; ++j) {
             AdjAcc &a0 = acc[2 * j], &a1 = acc[2 * j + 1];

@@ -105,6 +105,7 @@ struct BuildArgs {
     int n_atoms;
     double r_list0;   // rc + max|offset| (+ margin)
     double r_near0;   // r_split + max|offset| (+ margin)
+    double r_inner0;  // cutoff - max|offset| (- margin): inner entries lie within r_inner0 - rho
 };
 
 // Visit every candidate image of atom j for a region; f(dist2, rel) per image.
@@ -185,18 +186,22 @@ __global__ void __launch_bounds__(kBuildThreads)
     if (region >= n_regions) return;
     const RegionInfo r = regs[region];
     const double rl = a.r_list0 + r.rho, rn = a.r_near0 + r.rho, rn2 = rn * rn;
-    int near = 0, total = 0;
+    const double ri = a.r_inner0 - r.rho, ri2 = ri > 0 ? ri * ri : 0.0;
+    int near = 0, inner = 0, total = 0;
     for (int j = threadIdx.x; j < a.n_atoms; j += kBuildThreads)
         for_each_image(a, r, j, rl, [&](double q, double, double, double) {
             ++total;
             near += q < rn2;
+            inner += q >= rn2 && q < ri2;
         });
     __shared__ int sh[128];
-    int pa, pb, ta, tb;
+    int pa, pb, ta, tb, pc, pd, tc, td;
     block_scan2<kBuildThreads>(near, total, pa, pb, ta, tb, sh);
+    block_scan2<kBuildThreads>(inner, 0, pc, pd, tc, td, sh);
     if (threadIdx.x == 0) {
         regs[region].n_near = ta;
         regs[region].n_total = tb;
+        regs[region].n_inner = tc;
     }
 }
 
@@ -207,24 +212,30 @@ __global__ void __launch_bounds__(kBuildThreads)
     if (region >= n_regions) return;
     const RegionInfo r = regs[region];
     const double rl = a.r_list0 + r.rho, rn = a.r_near0 + r.rho, rn2 = rn * rn;
+    const double ri = a.r_inner0 - r.rho, ri2 = ri > 0 ? ri * ri : 0.0;
     __shared__ int sh[128];
-    int base_near = 0, base_far = r.n_near;
+    // entry order: near | far inner | far shell, atom-major inside each class
+    int base_near = 0, base_inner = r.n_near, base_shell = r.n_near + r.n_inner;
     for (int j0 = 0; j0 < a.n_atoms; j0 += kBuildThreads) {
         const int j = j0 + threadIdx.x;
-        int near = 0, far = 0;
+        int near = 0, inner = 0, shell = 0;
         if (j < a.n_atoms)
             for_each_image(a, r, j, rl, [&](double q, double, double, double) {
-                if (q < rn2) ++near; else ++far;
+                if (q < rn2) ++near;
+                else if (q < ri2) ++inner;
+                else ++shell;
             });
-        int pn, pf, tn, tf;
-        block_scan2<kBuildThreads>(near, far, pn, pf, tn, tf, sh);
+        int pn, pi, tn, ti, ps, pz, ts, tz;
+        block_scan2<kBuildThreads>(near, inner, pn, pi, tn, ti, sh);
+        block_scan2<kBuildThreads>(shell, 0, ps, pz, ts, tz, sh);
         if (j < a.n_atoms) {
-            int wn = base_near + pn, wf = base_far + pf;
+            int wn = base_near + pn, wi = base_inner + pi, ws = base_shell + ps;
             const int t = a.type[j];
             for_each_image(a, r, j, rl, [&](double q, double x, double y, double z) {
-                const int slot = q < rn2 ? wn++ : wf++;
-                const bool ok = q < rn2 ? slot < r.n_near : slot < r.n_total;
-                if (!ok) {
+                const int cls = q < rn2 ? 0 : (q < ri2 ? 1 : 2);
+                const int slot = cls == 0 ? wn++ : (cls == 1 ? wi++ : ws++);
+                const int end = cls == 0 ? r.n_near : (cls == 1 ? r.n_near + r.n_inner : r.n_total);
+                if (slot >= end) {
                     atomicExch(status, DEV_BAD_LIST);
                     return;
                 }
@@ -234,9 +245,11 @@ __global__ void __launch_bounds__(kBuildThreads)
             });
         }
         base_near += tn;
-        base_far += tf;
+        base_inner += ti;
+        base_shell += ts;
     }
-    if (threadIdx.x == 0 && (base_near != r.n_near || base_far != r.n_total))
+    if (threadIdx.x == 0 && (base_near != r.n_near || base_inner != r.n_near + r.n_inner ||
+                             base_shell != r.n_total))
         atomicExch(status, DEV_BAD_LIST);
 }
 
@@ -259,6 +272,7 @@ static int build_lists(System *sys, RegionSet *rs, cudaStream_t stream) {
     // FP64 rounding of the distances (~1e-14 A).
     a.r_list0 = sys->cutoff + sys->max_offset + 1e-6;
     a.r_near0 = rs->r_split + sys->max_offset + 1e-6;
+    a.r_inner0 = sys->cutoff - sys->max_offset - 1e-6;
     const int n = rs->n_regions;
     if (!rs->d_info) VEXT_CUDA(cudaMalloc(&rs->d_info, sizeof(RegionInfo) * n));
     VEXT_CUDA(cudaMemcpyAsync(rs->d_info, rs->h_info.data(), sizeof(RegionInfo) * n,
@@ -305,7 +319,7 @@ int get_field_regions(System *sys, int size, int cb, double r_split, RegionSet *
     for (RegionSet *rs : sys->sets)
         if (rs->size == size && rs->bi * rs->bj * rs->bk == cb && rs->r_split == r_split) {
             if (rs->stale) {
-                for (auto &r : rs->h_info) r.n_near = r.n_total = 0;
+                for (auto &r : rs->h_info) r.n_near = r.n_total = r.n_inner = 0;
                 VEXT_TRY(build_lists(sys, rs, stream));
             }
             *out = rs;
@@ -352,7 +366,7 @@ int get_bin_regions(System *sys, double r_split, RegionSet **out, cudaStream_t s
     for (RegionSet *rs : sys->sets)
         if (rs->size == 0 && rs->r_split == r_split) {
             if (rs->stale) {
-                for (auto &r : rs->h_info) r.n_near = r.n_total = 0;
+                for (auto &r : rs->h_info) r.n_near = r.n_total = r.n_inner = 0;
                 VEXT_TRY(build_lists(sys, rs, stream));
             }
             *out = rs;

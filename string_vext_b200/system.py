@@ -223,11 +223,24 @@ class VextBatch:
         d, e = ctypes.c_int(), ctypes.c_int()
         _lib.check(self._lib.vext_batch_info(self.handle, ctypes.byref(a), ctypes.byref(b),
                                              ctypes.byref(c), ctypes.byref(d), ctypes.byref(e)))
-        adj = self.gradients is not None
-        shapes = ("256x2 dirs", "128x4 dirs") if adj else ("128x4 dirs", "256x2 dirs")
+        tuning = self.tuning()
+        name = next((t["name"] for t in tuning
+                     if t["shape"] == d.value and t["grid"] == e.value), None)
         return {"work_items": a.value, "poses": b.value, "list_bytes": c.value,
-                "shape": d.value, "cta_shape": shapes[d.value], "grid": e.value,
-                "adjoint": adj}
+                "shape": d.value, "cta_shape": name, "grid": e.value,
+                "adjoint": self.gradients is not None, "tuning": tuning}
+
+    def tuning(self) -> list:
+        """The autotuner's candidates: shape name (threads x directors per
+        thread[/CTAs-per-SM bound]), resident CTAs, sample time (ms)."""
+        m = 8
+        n = ctypes.c_int()
+        shapes, grids = (ctypes.c_int * m)(), (ctypes.c_int * m)()
+        ms, names = (ctypes.c_float * m)(), (ctypes.c_char_p * m)()
+        _lib.check(self._lib.vext_batch_tuning(self.handle, m, ctypes.byref(n), shapes, grids,
+                                               ms, names))
+        return [{"name": names[i].decode(), "shape": shapes[i], "grid": grids[i],
+                 "sample_ms": ms[i]} for i in range(min(n.value, m))]
 
     def close(self) -> None:
         if getattr(self, "handle", None):
