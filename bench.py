@@ -42,12 +42,12 @@ sys.path.insert(0, str(ROOT))
 FLOP_FWD = 16          # algorithmic FLOP per in-cutoff (site, image) pair, forward
 FLOP_FWD_ADJ = 28      # forward + adjoint
 METRIC = "Vext pose evals/s at <=1e-4 K vs FP64, fwd+adjoint evals/s; % FP32 peak"
-# dram__bytes_read.sum + dram__bytes_write.sum of one field_far_kernel launch on
+# dram__bytes_read.sum + dram__bytes_write.sum of one field_far2_kernel launch on
 # full_field, from an ncu capture (--set full) of `bench.py --profile field`.
-FAR_DRAM_BYTES_FULL_FIELD = 741_898_752 + 101_475_584
-# the same for one forward + adjoint batch_field_kernel launch on full_field
-# (`bench.py --profile adjoint`); None until captured.
-ADJ_DRAM_BYTES_FULL_FIELD = None
+FAR_DRAM_BYTES_FULL_FIELD = 743_810_048 + 100_710_144
+# the same for one forward + adjoint batch_field_kernel launch on full_field,
+# from an ncu capture (--set full) of `bench.py --profile adjoint`.
+ADJ_DRAM_BYTES_FULL_FIELD = 424_774_656 + 353_256_704
 CPU_CENTERS_PER_CORE_S = 900.0   # reference driver throughput estimate used to size the sample
 
 
