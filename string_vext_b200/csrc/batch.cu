@@ -576,7 +576,7 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
         int occ = 0;
         VEXT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bk.fn, bk.threads, smem));
         if (occ < 1) continue;
-        cands[n_cands++] = {k, sms * occ};
+        if (n_cands < kMaxCandidates) cands[n_cands++] = {k, sms * occ};
         if (occ >= 2 && n_cands < kMaxCandidates) cands[n_cands++] = {k, sms * (occ / 2)};
     }
     if (n_cands == 0) return fail(VEXT_ERR_CAPACITY, "batch kernel does not fit an SM");

@@ -233,7 +233,7 @@ class VextBatch:
     def tuning(self) -> list:
         """The autotuner's candidates: shape name (threads x directors per
         thread[/CTAs-per-SM bound]), resident CTAs, sample time (ms)."""
-        m = 8
+        m = 16
         n = ctypes.c_int()
         shapes, grids = (ctypes.c_int * m)(), (ctypes.c_int * m)()
         ms, names = (ctypes.c_float * m)(), (ctypes.c_char_p * m)()
