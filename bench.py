@@ -439,7 +439,46 @@ def secondary_measurements(args, system, case, size, axes, poses, pairs, far_pai
     if not args.no_batch:
         out["batch"] = bench_batch(args, size, axes, device, stream, adjoint=False)
         out["batch_fwd_adjoint"] = bench_batch(args, size, axes, device, stream, adjoint=True)
+        out["string_batch_fwd_adjoint"] = bench_string_batch(device, stream)
     return out
+
+
+def bench_string_batch(device, stream):
+    """Forward + adjoint of 100 String paths (32-96 images, one per framework x
+    guest of the batched workload) in one launch (vext_pose_batch_run)."""
+    import torch
+    from string_vext_b200 import synth
+    from string_vext_b200.system import VextPoseBatch, VextSystem
+    cases = synth.batch_frameworks()
+    paths = synth.string_paths_batch(cases, n_paths=len(cases))
+    centers = np.concatenate([f @ np.asarray(cases[k]["cell"], dtype=float) for k, f, _ in paths])
+    quats = np.concatenate([q for _, _, q in paths])
+    counts = [len(f) for _, f, _ in paths]          # path p belongs to system p
+    t0 = time.perf_counter()
+    systems = [VextSystem(c) for c in cases]
+    batch = VextPoseBatch(systems, counts)
+    setup_s = time.perf_counter() - t0
+    dev = dict(dtype=torch.float64, device=device)
+    n = len(centers)
+    c, q = torch.tensor(centers, **dev), torch.tensor(quats, **dev)
+    e, gc, gq = torch.empty(n, **dev), torch.empty((n, 3), **dev), torch.empty((n, 4), **dev)
+
+    def step():
+        batch.run(c, q, e, gc, gq, stream=stream)
+
+    for _ in range(3):
+        step()
+    reps = 20
+    ms = timed_region(step, reps, stream) / reps
+    batch.check()
+    result = {"value": n / (ms * 1e-3), "unit": "poses/s", "ms_per_batch": ms, "paths": len(paths),
+              "poses": n, "systems": len(systems), "setup_s": setup_s,
+              "workload": "100 seeded String paths (32-96 images, random quaternions) over "
+                          "50 frameworks x 2 guests, one launch per evaluation"}
+    batch.close()
+    for s_ in systems:
+        s_.close()
+    return result
 
 
 def bench_batch(args, size, axes, device, stream, adjoint=False):

@@ -301,6 +301,32 @@ VEXT_API int vext_batch_tuning(vext_batch batch, int max_candidates, int *n_cand
                                int *shapes, int *grids, float *ms, const char **names);
 
 /* ------------------------------------------------------------------------ */
+/* Batched poses of many systems in ONE launch: the String paths of a batch of
+ * frameworks x guests, forward + adjoint every iteration.  The poses of
+ * systems[k] are rows [pose_offsets[k], pose_offsets[k+1]) (host array of
+ * n_systems + 1 entries, pose_offsets[0] = 0) of the DEVICE arrays given to
+ * vext_pose_batch_run: centers [n][3] Cartesian A, quats [n][4] (w, x, y, z);
+ * outputs as vext_pose_energy_grad (energy [n], grad_center [n][3], tangent
+ * grad_quat [n][4], grad_director [n][3], any may be NULL).  One warp per
+ * pose over its bin list: FP64 near pairs, FP32 far pairs with FP64-flushed
+ * partial sums, poses in the refinement band recomputed in FP64 (mixed mode;
+ * VEXT_MODE_FP64 evaluates every pair in FP64).  Replaces the per-image
+ * String energy kernels run once per path (global.h:1071-1128, 1141-1325);
+ * no reference counterpart for the batching.  The systems must outlive the
+ * batch and must not be invalidated while it exists. */
+typedef struct vext_pose_batch_s *vext_pose_batch;
+
+VEXT_API int vext_pose_batch_create(int n_systems, const vext_system *systems,
+                                    const int64_t *pose_offsets, const vext_options *opt,
+                                    vext_pose_batch *out);
+VEXT_API int vext_pose_batch_run(vext_pose_batch batch, const double *centers,
+                                 const double *quats, double *energy, double *grad_center,
+                                 double *grad_quat, double *grad_director, void *stream);
+/* Wait for the device; report a non-finite input or a device error. */
+VEXT_API int vext_pose_batch_status(vext_pose_batch batch);
+VEXT_API int vext_pose_batch_destroy(vext_pose_batch batch);
+
+/* ------------------------------------------------------------------------ */
 /* Diagnostics. */
 
 /* Non-tensor FP32 FMA throughput of the current device (FLOP/s, FMA = 2),

@@ -136,6 +136,15 @@ def load() -> ctypes.CDLL:
                                       ctypes.POINTER(ci), ctypes.POINTER(ctypes.c_float),
                                       ctypes.POINTER(ctypes.c_char_p)]
     lib.vext_batch_tuning.restype = ci
+    lib.vext_pose_batch_create.argtypes = [ci, vp, vp, ctypes.POINTER(Options),
+                                           ctypes.POINTER(vp)]
+    lib.vext_pose_batch_create.restype = ci
+    lib.vext_pose_batch_run.argtypes = [vp] + [vp] * 6 + [vp]
+    lib.vext_pose_batch_run.restype = ci
+    lib.vext_pose_batch_status.argtypes = [vp]
+    lib.vext_pose_batch_status.restype = ci
+    lib.vext_pose_batch_destroy.argtypes = [vp]
+    lib.vext_pose_batch_destroy.restype = ci
     lib.vext_batch_run.argtypes = [vp, vp]
     lib.vext_batch_run.restype = ci
     lib.vext_batch_status.argtypes = [vp]

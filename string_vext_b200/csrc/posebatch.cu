@@ -1,0 +1,322 @@
+// Forward + adjoint of many pose sets of different systems in ONE launch:
+// the String paths of a batch of frameworks x guests (each path a few dozen
+// images), evaluated every iteration.
+//
+// One warp per pose.  The pose's center is wrapped into its system's cell and
+// binned (the bin lists of system.cu, built at creation); the 32 lanes stride
+// over the bin's list: near entries in FP64 from hi + lo with the contact
+// floor, far entries in FP32 (reciprocal of d^2 per pair, cubed) with
+// per-lane FP32 partials flushed into FP64 every 16 entries.  The seven sums
+// (E, dE/dsite for both sites) are reduced over the warp; a pose whose energy
+// falls in the refinement band is recomputed entirely in FP64 by the same
+// warp.  Outputs as vext_pose_energy_grad: E, dE/dcenter, tangent dE/dq,
+// dE/du.  Pair term and forces as in pose.cu.
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace vext {
+
+struct PoseBatchSys {
+    Mat3 H, Hinv;
+    double rc2;
+    float rc2f;
+    double off0, off1;
+    int nb0, nb1, nb2;
+    const RegionInfo *regs;
+    const float4 *hi, *lo;
+    const double *td;   // (c12, c6, shift, floor2) per type
+    const float4 *tf;
+};
+
+struct PoseBatchArgs {
+    const PoseBatchSys *sys;
+    const long long *offsets;   // [n_systems + 1]: poses of system k
+    int n_systems;
+    long long n;
+    const double *centers, *quats;
+    double *energy, *gc, *gq, *gu;
+    double band_lo, band_hi;
+    int *status;
+};
+
+// Sums of one pose over its bin list: v = (E, dE/dsite0 [3], dE/dsite1 [3]),
+// lane-partial (reduced by the caller).  FAR64 evaluates the far entries in
+// FP64 too (refinement).
+template <bool FAR64>
+__device__ __forceinline__ void pose_sums(const PoseBatchSys &y, const RegionInfo &r,
+                                          const double (&sd)[2][3], int lane, double (&v)[7]) {
+    for (int e = lane; e < (FAR64 ? r.n_total : r.n_near); e += 32) {
+        const float4 h = y.hi[r.off + e], l = y.lo[r.off + e];
+        const double x = (double)h.x + (double)l.x, yy = (double)h.y + (double)l.y,
+                     z = (double)h.z + (double)l.z;
+        const int t = __float_as_int(h.w);
+        const double c12 = y.td[4 * t], c6 = y.td[4 * t + 1], shift = y.td[4 * t + 2],
+                     fl = y.td[4 * t + 3];
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const double dx = sd[s][0] - x, dy = sd[s][1] - yy, dz = sd[s][2] - z;
+            const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
+            if (d2 >= y.rc2) continue;
+            const double s2 = d2 < fl ? fl : d2;
+            const double i2 = 1.0 / s2;
+            const double i6 = i2 * i2 * i2;
+            v[0] += fma(i6, fma(c12, i6, -c6), shift);
+            if (d2 > fl) {
+                // dE/dsite = 2 dE/d(d2) (site - x),  dE/d(d2) = i2 i6 (3 c6 - 6 c12 i6)
+                const double w = i2 * i6 * fma(-12.0 * c12, i6, 6.0 * c6);
+                v[1 + 3 * s] = fma(w, dx, v[1 + 3 * s]);
+                v[2 + 3 * s] = fma(w, dy, v[2 + 3 * s]);
+                v[3 + 3 * s] = fma(w, dz, v[3 + 3 * s]);
+            }
+        }
+    }
+    if (FAR64) return;
+    float sf[2][3];
+#pragma unroll
+    for (int s = 0; s < 2; ++s)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) sf[s][k] = (float)sd[s][k];
+    const int n_far = r.n_total - r.n_near;
+    const int mine = n_far > lane ? (n_far - lane + 31) / 32 : 0;   // this lane's far entries
+    for (int i0 = 0; i0 < mine; i0 += 16) {
+        float fv[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        const int i1 = min(i0 + 16, mine);
+        for (int i = i0; i < i1; ++i) {
+            const float4 h = y.hi[r.off + r.n_near + lane + 32 * i];
+            const float4 tp = y.tf[__float_as_int(h.w)];   // (c12, c6, shift, floor2)
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                const float dx = sf[s][0] - h.x, dy = sf[s][1] - h.y, dz = sf[s][2] - h.z;
+                const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                float n1;
+                asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(n1) : "f"(d2));
+                const float m = d2 < y.rc2f ? 1.f : 0.f;
+                const float n3 = n1 * n1 * n1 * m;
+                fv[0] += fmaf(n3, fmaf(tp.x, n3, -tp.y), m * tp.z);
+                // far pairs lie beyond r_split: no contact floor
+                const float w = (n1 * n3) * fmaf(-12.f * tp.x, n3, 6.f * tp.y);
+                fv[1 + 3 * s] = fmaf(w, dx, fv[1 + 3 * s]);
+                fv[2 + 3 * s] = fmaf(w, dy, fv[2 + 3 * s]);
+                fv[3 + 3 * s] = fmaf(w, dz, fv[3 + 3 * s]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 7; ++k) v[k] += (double)fv[k];
+    }
+}
+
+__device__ __forceinline__ void warp_reduce7(double (&v)[7]) {
+#pragma unroll
+    for (int k = 0; k < 7; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+}
+
+__global__ void __launch_bounds__(256) pose_batch_kernel(PoseBatchArgs a) {
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < a.n;
+         p += nwarps) {
+        // system of pose p: offsets[k] <= p < offsets[k + 1]
+        int lo = 0, hi = a.n_systems - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (a.offsets[mid] <= p) lo = mid;
+            else hi = mid - 1;
+        }
+        const PoseBatchSys &y = a.sys[lo];
+        const double *q = a.quats + 4 * p;
+        const double nq = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+        bool ok = isfinite(nq) && nq > 0;
+        const double qw = ok ? q[0] / nq : 1.0, qx = ok ? q[1] / nq : 0.0,
+                     qy = ok ? q[2] / nq : 0.0, qz = ok ? q[3] / nq : 0.0;
+        const double u[3] = {1.0 - 2.0 * (qy * qy + qz * qz), 2.0 * (qx * qy + qw * qz),
+                             2.0 * (qx * qz - qw * qy)};
+        const double c0 = a.centers[3 * p], c1 = a.centers[3 * p + 1], c2 = a.centers[3 * p + 2];
+        double f[3];
+        int b[3];
+        const int nb[3] = {y.nb0, y.nb1, y.nb2};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            double w = c0 * y.Hinv.m[k] + c1 * y.Hinv.m[3 + k] + c2 * y.Hinv.m[6 + k];
+            ok = ok && isfinite(w);
+            w = isfinite(w) ? w - floor(w) : 0.0;
+            if (w >= 1.0) w = 0.0;
+            f[k] = w;
+            b[k] = min(nb[k] - 1, (int)(w * nb[k]));
+        }
+        if (!ok && lane == 0) atomicExch(a.status, DEV_BAD_INPUT);
+        const RegionInfo r = y.regs[(b[0] * y.nb1 + b[1]) * y.nb2 + b[2]];
+        double cx, cy, cz;
+        frac_to_cart(y.H, f[0] - r.of[0], f[1] - r.of[1], f[2] - r.of[2], cx, cy, cz);
+        double sd[2][3];
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const double off = s ? y.off1 : y.off0;
+            sd[s][0] = cx + off * u[0];
+            sd[s][1] = cy + off * u[1];
+            sd[s][2] = cz + off * u[2];
+        }
+        double v[7] = {0, 0, 0, 0, 0, 0, 0};
+        pose_sums<false>(y, r, sd, lane, v);
+        warp_reduce7(v);
+        if (v[0] > a.band_lo && v[0] < a.band_hi) {   // warp-uniform: every lane holds the sum
+#pragma unroll
+            for (int k = 0; k < 7; ++k) v[k] = 0.0;
+            pose_sums<true>(y, r, sd, lane, v);
+            warp_reduce7(v);
+        }
+        if (lane == 0) {
+            if (a.energy) a.energy[p] = v[0];
+            double gu[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                if (a.gc) a.gc[3 * p + k] = v[1 + k] + v[4 + k];
+                gu[k] = y.off0 * v[1 + k] + y.off1 * v[4 + k];
+                if (a.gu) a.gu[3 * p + k] = gu[k];
+            }
+            if (a.gq) {
+                // dE/dq = J(q)^T dE/du, projected on the tangent space of |q| = 1
+                double g[4];
+                g[0] = 2 * qz * gu[1] - 2 * qy * gu[2];
+                g[1] = 2 * qy * gu[1] + 2 * qz * gu[2];
+                g[2] = -4 * qy * gu[0] + 2 * qx * gu[1] - 2 * qw * gu[2];
+                g[3] = -4 * qz * gu[0] + 2 * qw * gu[1] + 2 * qx * gu[2];
+                const double dot = g[0] * qw + g[1] * qx + g[2] * qy + g[3] * qz;
+                const double inv = ok ? 1.0 / nq : 0.0;
+                a.gq[4 * p + 0] = (g[0] - dot * qw) * inv;
+                a.gq[4 * p + 1] = (g[1] - dot * qx) * inv;
+                a.gq[4 * p + 2] = (g[2] - dot * qy) * inv;
+                a.gq[4 * p + 3] = (g[3] - dot * qz) * inv;
+            }
+        }
+    }
+}
+
+}  // namespace vext
+
+using namespace vext;
+
+struct vext_pose_batch_s {
+    std::vector<vext_system> systems;
+    long long n = 0;
+    int n_systems = 0;
+    Options opt;
+    PoseBatchSys *d_sys = nullptr;
+    long long *d_offsets = nullptr;
+    int *d_status = nullptr;
+    ~vext_pose_batch_s() {
+        cudaFree(d_sys);
+        cudaFree(d_offsets);
+        cudaFree(d_status);
+    }
+};
+
+extern "C" int vext_pose_batch_create(int n_systems, const vext_system *systems,
+                                      const int64_t *pose_offsets, const vext_options *opt,
+                                      vext_pose_batch *out) {
+    if (!out || n_systems < 1 || !systems || !pose_offsets)
+        return fail(VEXT_ERR_ARGUMENT, "bad pose batch arguments");
+    *out = nullptr;
+    if (pose_offsets[0] != 0) return fail(VEXT_ERR_ARGUMENT, "pose_offsets[0] must be 0");
+    for (int k = 0; k < n_systems; ++k) {
+        if (!systems[k]) return fail(VEXT_ERR_ARGUMENT, "null system %d", k);
+        if (pose_offsets[k + 1] < pose_offsets[k])
+            return fail(VEXT_ERR_ARGUMENT, "pose_offsets must not decrease");
+    }
+    auto *b = new vext_pose_batch_s();
+    std::unique_ptr<vext_pose_batch_s> guard(b);
+    b->systems.assign(systems, systems + n_systems);
+    b->n_systems = n_systems;
+    b->n = pose_offsets[n_systems];
+    b->opt = resolve_options(opt);
+    if (b->opt.mode != VEXT_MODE_MIXED && b->opt.mode != VEXT_MODE_FP64)
+        return fail(VEXT_ERR_ARGUMENT, "unknown precision mode %d", b->opt.mode);
+    const double r_split = b->opt.mode == VEXT_MODE_FP64 ? 1e30 : b->opt.r_split;
+    int dev = 0;
+    VEXT_CUDA(cudaGetDevice(&dev));
+    std::vector<PoseBatchSys> hs(n_systems);
+    for (int k = 0; k < n_systems; ++k) {
+        System *sys = &systems[k]->sys;
+        if (sys->device != dev)
+            return fail(VEXT_ERR_ARGUMENT, "system %d lives on another device", k);
+        std::lock_guard<std::mutex> lock(sys->lock);
+        RegionSet *rs = nullptr;
+        VEXT_TRY(get_bin_regions(sys, r_split, &rs, sys->stream));
+        PoseBatchSys &y = hs[k];
+        y.H = sys->H;
+        y.Hinv = sys->Hinv;
+        y.rc2 = sys->cutoff * sys->cutoff;
+        y.rc2f = (float)y.rc2;
+        y.off0 = sys->offsets[0];
+        y.off1 = sys->offsets[1];
+        y.nb0 = rs->nb[0];
+        y.nb1 = rs->nb[1];
+        y.nb2 = rs->nb[2];
+        y.regs = rs->d_info;
+        y.hi = rs->d_hi;
+        y.lo = rs->d_lo;
+        y.td = sys->d_td;
+        y.tf = sys->d_tf;
+    }
+    std::vector<long long> offs(pose_offsets, pose_offsets + n_systems + 1);
+    VEXT_CUDA(cudaMalloc(&b->d_sys, sizeof(PoseBatchSys) * n_systems));
+    VEXT_CUDA(cudaMemcpy(b->d_sys, hs.data(), sizeof(PoseBatchSys) * n_systems,
+                         cudaMemcpyHostToDevice));
+    VEXT_CUDA(cudaMalloc(&b->d_offsets, sizeof(long long) * (n_systems + 1)));
+    VEXT_CUDA(cudaMemcpy(b->d_offsets, offs.data(), sizeof(long long) * (n_systems + 1),
+                         cudaMemcpyHostToDevice));
+    VEXT_CUDA(cudaMalloc(&b->d_status, sizeof(int)));
+    VEXT_CUDA(cudaMemset(b->d_status, 0, sizeof(int)));
+    *out = guard.release();
+    return 0;
+}
+
+extern "C" int vext_pose_batch_run(vext_pose_batch b, const double *centers, const double *quats,
+                                   double *energy, double *grad_center, double *grad_quat,
+                                   double *grad_director, void *stream) {
+    if (!b) return fail(VEXT_ERR_ARGUMENT, "null pose batch");
+    if (b->n == 0) return 0;
+    if (!centers || !quats) return fail(VEXT_ERR_ARGUMENT, "centers and quaternions required");
+    PoseBatchArgs a;
+    a.sys = b->d_sys;
+    a.offsets = b->d_offsets;
+    a.n_systems = b->n_systems;
+    a.n = b->n;
+    a.centers = centers;
+    a.quats = quats;
+    a.energy = energy;
+    a.gc = grad_center;
+    a.gq = grad_quat;
+    a.gu = grad_director;
+    const bool band = b->opt.mode == VEXT_MODE_MIXED && b->opt.band_hi > b->opt.band_lo;
+    a.band_lo = band ? b->opt.band_lo : 0.0;
+    a.band_hi = band ? b->opt.band_hi : 0.0;
+    a.status = b->d_status;
+    const long long blocks = std::min<long long>((b->n + 7) / 8, 148LL * 16);
+    pose_batch_kernel<<<(int)blocks, 256, 0, (cudaStream_t)stream>>>(a);
+    VEXT_CUDA(cudaGetLastError());
+    return 0;
+}
+
+extern "C" int vext_pose_batch_status(vext_pose_batch b) {
+    if (!b) return fail(VEXT_ERR_ARGUMENT, "null pose batch");
+    int h = 0;
+    VEXT_CUDA(cudaDeviceSynchronize());
+    VEXT_CUDA(cudaMemcpy(&h, b->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) {
+        VEXT_CUDA(cudaMemset(b->d_status, 0, sizeof(int)));
+        if (h == DEV_BAD_INPUT) return fail(VEXT_ERR_ARGUMENT, "non-finite pose center or zero quaternion");
+        return fail(VEXT_ERR_TIMEOUT, "device status %d", h);
+    }
+    return 0;
+}
+
+extern "C" int vext_pose_batch_destroy(vext_pose_batch b) {
+    delete b;
+    return 0;
+}

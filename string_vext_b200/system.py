@@ -252,3 +252,46 @@ class VextBatch:
             self.close()
         except Exception:
             pass
+
+
+class VextPoseBatch:
+    """Poses of many systems (e.g. one String path per framework x guest)
+    forward + adjoint in one launch (``vext_pose_batch_create``).  ``counts[k]``
+    poses belong to ``systems[k]``; ``run`` takes CUDA float64 tensors with the
+    poses of all systems stacked in that order."""
+
+    def __init__(self, systems, counts, mode: int = _lib.VEXT_MODE_MIXED, **opts):
+        self._lib = _lib.load()
+        self.systems = list(systems)           # kept alive: the batch points into them
+        offsets = np.zeros(len(self.systems) + 1, dtype=np.int64)
+        offsets[1:] = np.cumsum(np.asarray(counts, dtype=np.int64))
+        self.n = int(offsets[-1])
+        handles = (ctypes.c_void_p * len(self.systems))(*[s.handle.value for s in self.systems])
+        opt = _lib.options(mode, **opts)
+        handle = ctypes.c_void_p()
+        _lib.check(self._lib.vext_pose_batch_create(len(self.systems), handles,
+                                                    _lib.ptr(offsets), ctypes.byref(opt),
+                                                    ctypes.byref(handle)))
+        self.handle = handle
+
+    def run(self, centers, quats, energy, grad_center=None, grad_quat=None,
+            grad_director=None, stream=None) -> None:
+        h = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        _lib.check(self._lib.vext_pose_batch_run(self.handle, _lib.ptr(centers), _lib.ptr(quats),
+                                                 _lib.ptr(energy), _lib.ptr(grad_center),
+                                                 _lib.ptr(grad_quat), _lib.ptr(grad_director),
+                                                 h))
+
+    def check(self) -> None:
+        _lib.check(self._lib.vext_pose_batch_status(self.handle))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self._lib.vext_pose_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
