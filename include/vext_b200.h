@@ -266,6 +266,27 @@ VEXT_API int vext_string_run(vext_system sys, int n_images, double *path, double
                              vext_string_result *result);
 
 /* ------------------------------------------------------------------------ */
+/* Transition-state-theory post-processing of a String path (host only).
+ * frac [n][3] fractional image positions, energy [n] in K, cell the
+ * row-vector cell matrix (3 x 3), hop_A the hopping length (the cell length
+ * along the transport axis), temperature in K, mass in g/mol.
+ *   vext_tst_diffusivity: the hopping diffusivity D0 (m^2/s) the String
+ *     program prints: 0.5 L^2 sqrt(kT/(2 pi m)) exp(-Vmax/T) / trapz over
+ *     the Cartesian arc length of exp(-V/T) (capped at exp(-600))
+ *     (native/string/source_code/RC_main.cu:2485-2527; the standalone
+ *     diffusivity.c:117-172 computes the same without the cap).
+ *   vext_tst_log_score: log D with the shifted-energy trapezoid in log
+ *     space; *valid = 0 for invalid inputs or a non-finite result
+ *     (legacy_policy.h:21-49).  The reference keeps the initial path when its
+ *     score is valid and higher than the final one's (legacy_policy.h:50-52). */
+VEXT_API int vext_tst_diffusivity(int n, const double *frac, const double *energy,
+                                  const double *cell, double hop_A, double temperature,
+                                  double mass_g_mol, double *d0);
+VEXT_API int vext_tst_log_score(int n, const double *frac, const double *energy,
+                                const double *cell, double temperature, double mass_g_mol,
+                                double hop_A, int *valid, double *log_d);
+
+/* ------------------------------------------------------------------------ */
 /* Batched fields: many systems (frameworks x guests of uneven sizes and cell
  * shapes) in one persistent launch over a work queue of (system, region,
  * 32-director block) items, longest first, captured in a CUDA graph.  The

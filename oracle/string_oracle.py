@@ -140,3 +140,32 @@ def iteration(case, s0, hf=1e-4, ha=PI / 180, direction=1, smooth=1e-4, rounding
         col = np.where(col > 2 * PI, col - 2 * PI, np.where(col < 0, col + 2 * PI, col))
         new[:, k] = col
     return new, False, (mt, mr), e0
+
+
+def tst_diffusivity(frac, energy, cell, hop_A, temperature, mass_g_mol):
+    """The String program's hopping diffusivity (RC_main.cu:2485-2527) restated:
+    Cartesian arc length in m, trapezoid of exp(-V/T) capped at exp(-600),
+    D0 = 0.5 L^2 sqrt(kT / (2 pi m)) exp(-Vmax / T) / trapz."""
+    import math
+    frac = np.asarray(frac, dtype=float)
+    cell = np.asarray(cell, dtype=float)
+    A, B, C = cell[:, 0], cell[:, 1], cell[:, 2]
+    T = temperature
+    xs = [(f[0] * A[0] + f[1] * A[1] + f[2] * A[2]) * 1e-10 for f in frac]
+    ys = [(f[0] * B[0] + f[1] * B[1] + f[2] * B[2]) * 1e-10 for f in frac]
+    zs = [(f[0] * C[0] + f[1] * C[1] + f[2] * C[2]) * 1e-10 for f in frac]
+    s = [0.0]
+    for i in range(1, len(frac)):
+        s.append(s[-1] + math.sqrt((xs[i] - xs[i - 1]) ** 2 + (ys[i] - ys[i - 1]) ** 2
+                                   + (zs[i] - zs[i - 1]) ** 2))
+    w = [math.exp(-6e2) if e / T > 6e2 else math.exp(-e / T) for e in energy]
+    integral = 0.0
+    for i in range(1, len(frac)):
+        integral = integral + (s[i] - s[i - 1]) * (w[i] + w[i - 1]) / 2
+    vmax = energy[0]
+    for e in energy:
+        if e > vmax:
+            vmax = e
+    return (0.5 * (hop_A * 1e-10) ** 2
+            * math.sqrt((1.38e-23 * T) / (2 * PI * (mass_g_mol / 1e3 / 6.02214076e23)))
+            * (math.exp(-vmax / T) / integral))

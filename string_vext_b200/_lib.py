@@ -145,6 +145,12 @@ def load() -> ctypes.CDLL:
     lib.vext_pose_batch_status.restype = ci
     lib.vext_pose_batch_destroy.argtypes = [vp]
     lib.vext_pose_batch_destroy.restype = ci
+    lib.vext_tst_diffusivity.argtypes = [ci, vp, vp, vp, cd, cd, cd,
+                                         ctypes.POINTER(ctypes.c_double)]
+    lib.vext_tst_diffusivity.restype = ci
+    lib.vext_tst_log_score.argtypes = [ci, vp, vp, vp, cd, cd, cd, ctypes.POINTER(ci),
+                                       ctypes.POINTER(ctypes.c_double)]
+    lib.vext_tst_log_score.restype = ci
     lib.vext_batch_run.argtypes = [vp, vp]
     lib.vext_batch_run.restype = ci
     lib.vext_batch_status.argtypes = [vp]

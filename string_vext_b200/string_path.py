@@ -43,6 +43,27 @@ def run_string(system, path, mode: int = _lib.VEXT_MODE_MIXED, **params):
     return path, energy, result.as_dict()
 
 
+def path_selection(case, initial, initial_energy, final, final_energy, direction: int,
+                   temperature: float | None = None, mass_g_mol: float | None = None) -> dict:
+    """The reference's end-of-run summary (RC_main.cu:2485-2552): hopping
+    diffusivity of the final path, log-domain scores of the initial and final
+    paths and the chosen one (the initial path when its score is valid and
+    higher).  Temperature and guest mass default to the case's."""
+    from .tst import choose_initial, diffusivity, hop_length, log_score
+    T = float(case["temperature"] if temperature is None else temperature)
+    mass = float(case["total_mass"] if mass_g_mol is None else mass_g_mol)
+    hop = hop_length(case, direction)
+    s_init = log_score(initial, initial_energy, case["cell"], T, mass, hop)
+    s_final = log_score(final, final_energy, case["cell"], T, mass, hop)
+    use_initial = choose_initial(s_init, s_final)
+    return {"diffusivity_final_m2_s": diffusivity(final, final_energy, case["cell"], hop, T, mass),
+            "log_d_initial": s_init[1] if s_init[0] else None,
+            "log_d_final": s_final[1] if s_final[0] else None,
+            "chosen": "initial" if use_initial else "final",
+            "peak_initial_K": float(np.max(initial_energy)),
+            "peak_final_K": float(np.max(final_energy))}
+
+
 def write_path(path_file, path, energy) -> None:
     """Seven ``%.17g`` columns per image, as the reference solver writes."""
     lines = [" ".join(f"{v:.17g}" for v in (*row, e)) for row, e in zip(path, energy)]

@@ -7,8 +7,9 @@ import pytest
 
 from oracle import string_oracle
 from string_vext_b200 import _lib, synth
-from string_vext_b200.string_path import (euler_from_quaternions, quaternions_from_euler,
-                                          read_initial, run_string, write_path)
+from string_vext_b200.string_path import (euler_from_quaternions, path_selection,
+                                          quaternions_from_euler, read_initial, run_string,
+                                          write_path)
 from string_vext_b200.system import VextSystem
 
 pytestmark = pytest.mark.gpu
@@ -76,6 +77,11 @@ def test_string_run_200_iterations_and_files(tmp_path):
     back = np.loadtxt(out)
     np.testing.assert_array_equal(back[:, :6], path)
     np.testing.assert_array_equal(back[:, 6], energy)
+    # end-of-run summary: diffusivity and the initial / final path choice
+    e0 = string_oracle.pose_energy(case, s)
+    summary = path_selection(case, s, e0, path, energy, direction=3)
+    assert summary["chosen"] in ("initial", "final")
+    assert summary["diffusivity_final_m2_s"] >= 0
     init = tmp_path / "initial.dat"
     init.write_text("\n".join("\t".join(f"{v:.17g}" for v in row) for row in path) + "\n")
     np.testing.assert_array_equal(read_initial(init, 64), path)
