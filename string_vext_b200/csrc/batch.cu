@@ -62,7 +62,7 @@ struct BatchArgs {
 // (pair.cuh); writes the energy and [dE/dc, tangent dE/du] of every pose.
 // Far entries come in two passes: inner (no cutoff mask, shift summed once
 // per entry) and shell.
-template <int CB, int G, int P, bool NEWTON, bool RCP1>
+template <int CB, int G, int P, bool NEWTON, bool RCP1, int UNROLL>
 __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSys &y,
                                                const RegionInfo &r, Stager &st, double *ed,
                                                const float4 *stf, const double *std4,
@@ -123,11 +123,11 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
                 plan.chunk(c, start, len, near);
                 const float4 *hb = st.hib + ((seq + c) % kStages) * kCH;
                 if (pass)
-                    far_chunk_adj<P, NEWTON, 16, true, RCP1>(hb, stf, len, g, ux, uy, uz, acc,
-                                                             shift_sum);
+                    far_chunk_adj<P, NEWTON, 16, true, RCP1, UNROLL>(hb, stf, len, g, ux, uy, uz,
+                                                                     acc, shift_sum);
                 else
-                    far_chunk_adj<P, NEWTON, 16, false, RCP1>(hb, stf, len, g, ux, uy, uz, acc,
-                                                              shift_sum);
+                    far_chunk_adj<P, NEWTON, 16, false, RCP1, UNROLL>(hb, stf, len, g, ux, uy,
+                                                                      uz, acc, shift_sum);
                 stage_next(st, plan, y.hi, y.lo, c, seq);
             }
             seq += plan.n_chunks;
@@ -144,7 +144,8 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
 }
 
 // ADJ: 0 = forward; forward + adjoint with the far reciprocal taken as
-// 1 = rcp(q) cubed (default), 2 = rcp(q^3) + Newton, 3 = rcp(q^3).
+// 1 = rcp(q) cubed (default), 2 = rcp(q^3) + Newton, 3 = rcp(q^3);
+// 5 = as 1 with the far entry loop unrolled twice.
 template <int CB, int G, int P, int MINB, int ADJ>
 __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
     constexpr int NT = CB * G, PP = P / 2;
@@ -186,8 +187,8 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
         double e[P];
         double gr[ADJ ? P : 1][6];
         if constexpr (ADJ) {
-            if (!batch_item_adj<CB, G, P, ADJ == 2, ADJ == 1>(a, y, r, st, ed, stf, std4, seq,
-                                                              cx, cy, cz, obase, e, gr))
+            if (!batch_item_adj<CB, G, P, ADJ == 2, ADJ == 1 || ADJ == 5, ADJ == 5 ? 2 : 1>(
+                    a, y, r, st, ed, stf, std4, seq, cx, cy, cz, obase, e, gr))
                 return;
         } else {
         // ---- near pairs (FP64)
@@ -361,7 +362,8 @@ static const BatchKernel kForwardKernels[] = {
 static const BatchKernel kAdjointKernels[] = {
     {batch_field_kernel<16, 16, 2, 2, 1>, 256, "256x2"},
     {batch_field_kernel<16, 8, 4, 2, 1>, 128, "128x4"},
-    {batch_field_kernel<16, 8, 4, 3, 1>, 128, "128x4/3"}};
+    {batch_field_kernel<16, 8, 4, 3, 1>, 128, "128x4/3"},
+    {batch_field_kernel<16, 16, 2, 2, 5>, 256, "256x2 unroll2"}};
 static const BatchKernel kAdjointNewtonKernels[] = {   // accuracy/speed study
     {batch_field_kernel<16, 16, 2, 2, 2>, 256, "256x2 rcp3+newton"},
     {batch_field_kernel<16, 8, 4, 2, 2>, 128, "128x4 rcp3+newton"}};

@@ -440,7 +440,7 @@ __device__ __forceinline__ void near_chunk_adj(const double *ed, const double *s
 // summed once per entry into shift_sum (the caller adds 2 x shift_sum, both
 // sites, to every energy).  FP32 partials over FLUSH entries are flushed into
 // the FP64 AdjAcc.
-template <int P, bool NEWTON, int FLUSH, bool MASK, bool RCP1 = true>
+template <int P, bool NEWTON, int FLUSH, bool MASK, bool RCP1 = true, int UNROLL = 1>
 __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *stf, int len,
                                               const FarGeom &g, const float2 (&ux)[P / 2],
                                               const float2 (&uy)[P / 2],
@@ -463,7 +463,7 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
             }
         }
         const int e1 = min(e0 + FLUSH, len);
-#pragma unroll 1
+#pragma unroll UNROLL
         for (int e = e0; e < e1; ++e) {
             const float4 h = hb[e];
             const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, -)
