@@ -436,10 +436,45 @@ def secondary_measurements(args, system, case, size, axes, poses, pairs, far_pai
                                "poses": n_pose, "workload": "random poses (center, quaternion), "
                                "same framework", "flop_per_pair": FLOP_FWD_ADJ}
     del cart, q, e, gc, gq
+    out["precision_study"] = precision_study(device)
     if not args.no_batch:
         out["batch"] = bench_batch(args, size, axes, device, stream, adjoint=False)
         out["batch_fwd_adjoint"] = bench_batch(args, size, axes, device, stream, adjoint=True)
         out["string_batch_fwd_adjoint"] = bench_string_batch(device, stream)
+    return out
+
+
+def precision_study(device):
+    """The precision study: naive FP32, FP32 compensated throughout (every pair
+    beyond 1 A in packed FP32 with FP64-flushed partials, no FP64 band) and the
+    default mixed field, each against the tiled FP64 oracle kernel, on
+    skewed_field (28 x 31 x 24 A, alpha/beta/gamma 75/85/110, 3000 atoms,
+    60^3 x 64: every pose has E > 0) and small_field (20^3 x 64: the workload
+    with E <= 0 poses)."""
+    from string_vext_b200 import _lib, synth
+    from string_vext_b200.orientation import normalized_directors, regular_pose_grid
+    from string_vext_b200.system import VextSystem
+    out = {}
+    for name, maker, size in (("skewed_field", synth.skewed_field, 60),
+                              ("small_field", synth.small_field, 20)):
+        _, axes = regular_pose_grid(size, 64)
+        axes = normalized_directors(axes)
+        res = {"workload": f"{name}: {size}^3 x 64"}
+        with VextSystem(maker()) as system:
+            exact = system.field(size, axes, mode=_lib.VEXT_MODE_FP64, energy=True,
+                                 orientation=False)["energy"]
+            res["fp64_oracle_ms"] = system.last_stats["kernel_ms"]
+            for label, mode, opts in (
+                    ("fp32_naive", _lib.VEXT_MODE_FP32_NAIVE, {}),
+                    ("fp32_compensated", _lib.VEXT_MODE_MIXED,
+                     {"r_split": 1.0, "band": (0.0, 0.0)}),
+                    ("mixed_default", _lib.VEXT_MODE_MIXED, {})):
+                got = system.field(size, axes, mode=mode, energy=True, orientation=False,
+                                   **opts)["energy"]
+                stats = error_stats(got, exact)
+                stats["kernel_ms"] = system.last_stats["kernel_ms"]
+                res[label] = stats
+        out[name] = res
     return out
 
 

@@ -129,8 +129,11 @@ enum {
                                 FP64 re-evaluation of poses whose energy lies in
                                 the refinement band                           */
     VEXT_MODE_FP64 = 1,      /* every pair in FP64 (the GPU oracle kernel)     */
-    VEXT_MODE_FP64_PLAIN = 2 /* fields only: the plain FP64 baseline kernel
+    VEXT_MODE_FP64_PLAIN = 2,/* fields only: the plain FP64 baseline kernel
                                 (one thread per pose, no staging)            */
+    VEXT_MODE_FP32_NAIVE = 3 /* fields only, precision study: the same plain
+                                loop in FP32 (FP32 positions, IEEE FP32
+                                division, one FP32 sum per pose)             */
 };
 
 typedef struct {

@@ -19,6 +19,7 @@ LIB_PATH = Path(os.environ.get("VEXT_B200_LIBRARY", PACKAGE / "lib" / "libvext_b
 VEXT_MODE_MIXED = 0
 VEXT_MODE_FP64 = 1
 VEXT_MODE_FP64_PLAIN = 2
+VEXT_MODE_FP32_NAIVE = 3
 
 STATUS = {0: "ok", 1: "bad sizes", 2: "CSR starts decreasing", 3: "CSR index out of range",
           4: "non-finite energy", 16: "CUDA error", 17: "device wait timeout",

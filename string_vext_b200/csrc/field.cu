@@ -22,6 +22,7 @@
 namespace vext {
 
 constexpr int kPlainVariant = 1 << 20;
+constexpr int kNaiveVariant = 1 << 21;
 
 struct FieldArgs {
     Mat3 H;
@@ -473,6 +474,44 @@ __global__ void __launch_bounds__(256) plain_fp64_kernel(FieldArgs a) {
     }
 }
 
+// The naive FP32 field (precision study): plain_fp64_kernel's loop in FP32 --
+// sites relative to the region origin rounded to FP32, entries from hi only,
+// IEEE FP32 division, one FP32 sum per pose over both sites.
+__global__ void __launch_bounds__(256) plain_fp32_kernel(FieldArgs a) {
+    const long long S3 = (long long)a.S * a.S * a.S;
+    const long long n = S3 * a.O;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long c = idx % S3;
+        const int o = (int)(idx / S3);
+        const int gi = (int)(c / ((long long)a.S * a.S)), gj = (int)((c / a.S) % a.S),
+                  gk = (int)(c % a.S);
+        const RegionInfo r = a.regs[region_of(a, gi, gj, gk)];
+        double cx, cy, cz;
+        frac_to_cart(a.H, (gi + .5) / a.S - r.of[0], (gj + .5) / a.S - r.of[1],
+                     (gk + .5) / a.S - r.of[2], cx, cy, cz);
+        const double ux = a.axes[3 * o], uy = a.axes[3 * o + 1], uz = a.axes[3 * o + 2];
+        float e = 0.f;
+        for (int s = 0; s < 2; ++s) {
+            const double off = s ? a.off1 : a.off0;
+            const float px = (float)(cx + off * ux), py = (float)(cy + off * uy),
+                        pz = (float)(cz + off * uz);
+            for (int k = 0; k < r.n_total; ++k) {
+                const float4 h = a.hi[r.off + k];
+                const float dx = px - h.x, dy = py - h.y, dz = pz - h.z;
+                const float d2 = dx * dx + dy * dy + dz * dz;
+                if (d2 >= a.rc2f) continue;
+                const float4 tp = a.tf[__float_as_int(h.w)];   // (c12, c6, shift, floor2)
+                const float s2 = d2 < tp.w ? tp.w : d2;
+                const float i2 = 1.0f / s2;
+                const float i6 = i2 * i2 * i2;
+                e += tp.x * i6 * i6 - tp.y * i6 + tp.z;
+            }
+        }
+        a.e64[idx] = (double)e;
+    }
+}
+
 // The plain FP64 forward + adjoint: plain_fp64_kernel plus, per in-cutoff
 // pair off the contact floor, dE/d(r^2) = (-6 c12 i6^2 + 3 c6 i6) i2 and the
 // site gradient 2 dE/d(r^2) (site - x); dE/dc = sum over sites, dE/du =
@@ -653,6 +692,11 @@ int launch_field(System *sys, const RegionSet *rs, int n_axes, const double *d_a
         VEXT_CUDA(cudaGetLastError());
         return 0;
     }
+    if (rs->r_split >= 1e29 && variant == kNaiveVariant) {            // naive FP32 (study)
+        plain_fp32_kernel<<<148 * 16, 256, 0, stream>>>(a);
+        VEXT_CUDA(cudaGetLastError());
+        return 0;
+    }
     if (rs->r_split >= 1e29) return launch_near(a, cb, 0, stream);   // FP64 oracle
     // near pairs are at most r_split + 2 (rho + max|offset|) apart
     double rho = 0;
@@ -695,10 +739,11 @@ static int field_device(System *sys, int size, int n_axes, const double *axes_ho
         return fail(VEXT_ERR_CAPACITY, "size^3 * n_axes must stay below 2^31");
     for (int k = 0; k < 3 * n_axes; ++k)
         if (!std::isfinite(axes_host[k])) return fail(VEXT_ERR_ARGUMENT, "non-finite director");
-    if (o.mode != VEXT_MODE_MIXED && o.mode != VEXT_MODE_FP64 && o.mode != VEXT_MODE_FP64_PLAIN)
+    if (o.mode != VEXT_MODE_MIXED && o.mode != VEXT_MODE_FP64 && o.mode != VEXT_MODE_FP64_PLAIN &&
+        o.mode != VEXT_MODE_FP32_NAIVE)
         return fail(VEXT_ERR_ARGUMENT, "unknown precision mode %d", o.mode);
     const int cb = o.cb == 32 ? 32 : 16;
-    const bool fp64 = o.mode == VEXT_MODE_FP64 || o.mode == VEXT_MODE_FP64_PLAIN;
+    const bool fp64 = o.mode != VEXT_MODE_MIXED;   // all-entry region lists
     const double r_split = fp64 ? 1e30 : o.r_split;
     RegionSet *rs = nullptr;
     VEXT_TRY(get_field_regions(sys, size, cb, r_split, &rs, stream));
@@ -714,7 +759,10 @@ static int field_device(System *sys, int size, int n_axes, const double *axes_ho
     const FieldArgs a = make_args(sys, rs, n_axes, sys->d_axes, sys->d_e64);
     VEXT_CUDA(cudaEventRecord(sys->ev[0], stream));
     VEXT_TRY(launch_field(sys, rs, n_axes, sys->d_axes, sys->d_e64, cb,
-                          o.mode == VEXT_MODE_FP64_PLAIN ? kPlainVariant : o.variant, stream));
+                          o.mode == VEXT_MODE_FP64_PLAIN   ? kPlainVariant
+                          : o.mode == VEXT_MODE_FP32_NAIVE ? kNaiveVariant
+                                                           : o.variant,
+                          stream));
     VEXT_CUDA(cudaEventRecord(sys->ev[1], stream));
     if (o.mode == VEXT_MODE_MIXED && o.band_hi > o.band_lo) {
         flag_kernel<<<592, 256, 0, stream>>>(sys->d_e64, (long long)n, o.band_lo, o.band_hi,

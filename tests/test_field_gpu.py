@@ -128,3 +128,20 @@ def test_periodicity_of_the_field():
                                          np.tile([1.0, 0, 0, 0], (len(centers), 1)),
                                          mode=FP64, grad=False)
     np.testing.assert_allclose(e1, e2, rtol=1e-10, atol=1e-8)
+
+
+def test_fp32_naive_mode_is_bounded_and_worse_than_mixed():
+    """The precision study's naive FP32 field (plain loop, FP32 sum) stays
+    within FP32 rounding of the oracle, and the mixed field is more accurate."""
+    case = synth.small_field()
+    centers, axes = grid(4)
+    ref = oracle.pose_energy(case, centers, axes)
+    with VextSystem(case) as system:
+        naive = system.field(4, axes, mode=_lib.VEXT_MODE_FP32_NAIVE, energy=True,
+                             orientation=False)["energy"]
+        mixed = system.field(4, axes, energy=True, orientation=False)["energy"]
+    assert np.isfinite(naive).all()
+    err_naive = np.abs(naive - ref) / np.maximum(np.abs(ref), 1.0)
+    err_mixed = np.abs(mixed - ref) / np.maximum(np.abs(ref), 1.0)
+    assert err_naive.max() < 1e-3
+    assert err_mixed.max() < 0.1 * err_naive.max()
