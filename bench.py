@@ -39,6 +39,8 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+from string_vext_b200 import ranks  # noqa: E402  (no CUDA work at import)
+
 FLOP_FWD = 16          # algorithmic FLOP per in-cutoff (site, image) pair, forward
 FLOP_FWD_ADJ = 28      # forward + adjoint
 METRIC = "Vext pose evals/s at <=1e-4 K vs FP64, fwd+adjoint evals/s; % FP32 peak"
@@ -217,7 +219,6 @@ def timed_region(fn, steps, stream):
 
 def run_ours(args, rank, world, local_rank):
     import torch
-    import torch.distributed as dist
     from string_vext_b200 import _lib
     from string_vext_b200.orientation import normalized_directors, regular_pose_grid
     from string_vext_b200.system import VextSystem
@@ -251,14 +252,10 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    ranks.barrier()
     with ClockSampler(local_rank) as clocks:
         ms_total = timed_region(step, args.steps, stream)
-    if world > 1:
-        t = torch.tensor([ms_total], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = ranks.max_over_ranks(ms_total, device)
     ms_step = ms_total / args.steps
     value = world * poses * args.steps / (ms_total * 1e-3)
     achieved = pairs * FLOP_FWD_ADJ / (ms_step * 1e-3)
@@ -290,8 +287,7 @@ def run_ours(args, rank, world, local_rank):
         extra.update(secondary_measurements(args, system, case, size, axes, poses, pairs,
                                             far_pairs, peak, stream, device, ms_step, energy,
                                             grad))
-    if world > 1:
-        dist.barrier()
+    ranks.barrier()
     if rank != 0:
         return
     cpu = None
@@ -614,20 +610,12 @@ def main():
     if args.profile:
         run_profile_case(args.profile)
         return
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local_rank = ranks.rank_info()
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
     if world > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local_rank))
+        ranks.init("nccl", local_rank)
     try:
         run_ours(args, rank, world, local_rank)
     finally:
