@@ -62,7 +62,7 @@ struct BatchArgs {
 // (pair.cuh); writes the energy and [dE/dc, tangent dE/du] of every pose.
 // Far entries come in two passes: inner (no cutoff mask, shift summed once
 // per entry) and shell.
-template <int CB, int G, int P, bool NEWTON, bool RCP1, int UNROLL>
+template <int CB, int G, int P, bool NEWTON, bool RCP1, int UNROLL, int FLUSH>
 __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSys &y,
                                                const RegionInfo &r, Stager &st, double *ed,
                                                const float4 *stf, const double *std4,
@@ -123,11 +123,11 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
                 plan.chunk(c, start, len, near);
                 const float4 *hb = st.hib + ((seq + c) % kStages) * kCH;
                 if (pass)
-                    far_chunk_adj<P, NEWTON, 16, true, RCP1, UNROLL>(hb, stf, len, g, ux, uy, uz,
-                                                                     acc, shift_sum);
+                    far_chunk_adj<P, NEWTON, FLUSH, true, RCP1, UNROLL>(hb, stf, len, g, ux, uy,
+                                                                        uz, acc, shift_sum);
                 else
-                    far_chunk_adj<P, NEWTON, 16, false, RCP1, UNROLL>(hb, stf, len, g, ux, uy,
-                                                                      uz, acc, shift_sum);
+                    far_chunk_adj<P, NEWTON, FLUSH, false, RCP1, UNROLL>(hb, stf, len, g, ux, uy,
+                                                                         uz, acc, shift_sum);
                 stage_next(st, plan, y.hi, y.lo, c, seq);
             }
             seq += plan.n_chunks;
@@ -145,7 +145,9 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
 
 // ADJ: 0 = forward; forward + adjoint with the far reciprocal taken as
 // 1 = rcp(q) cubed (default), 2 = rcp(q^3) + Newton, 3 = rcp(q^3);
-// 5 = as 1 with the far entry loop unrolled twice.
+// 5 = as 1 with the far entry loop unrolled twice; 6 / 7 = as 1 with the
+// FP32 gradient partials flushed every 16 / 64 entries instead of once per
+// 128-entry chunk.
 template <int CB, int G, int P, int MINB, int ADJ>
 __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
     constexpr int NT = CB * G, PP = P / 2;
@@ -187,7 +189,8 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
         double e[P];
         double gr[ADJ ? P : 1][6];
         if constexpr (ADJ) {
-            if (!batch_item_adj<CB, G, P, ADJ == 2, ADJ == 1 || ADJ == 5, ADJ == 5 ? 2 : 1>(
+            if (!batch_item_adj<CB, G, P, ADJ == 2, ADJ == 1 || ADJ >= 5,
+                                ADJ == 5 ? 2 : 1, ADJ == 6 ? 16 : ADJ == 7 ? 64 : 128>(
                     a, y, r, st, ed, stf, std4, seq, cx, cy, cz, obase, e, gr))
                 return;
         } else {
@@ -370,17 +373,27 @@ static const BatchKernel kAdjointNewtonKernels[] = {   // accuracy/speed study
 static const BatchKernel kAdjointRcp3Kernels[] = {     // accuracy/speed study
     {batch_field_kernel<16, 16, 2, 2, 3>, 256, "256x2 rcp3"},
     {batch_field_kernel<16, 8, 4, 2, 3>, 128, "128x4 rcp3"}};
-constexpr int kMaxCandidates = 8;
+static const BatchKernel kAdjointFlush16Kernels[] = {   // accuracy/speed study
+    {batch_field_kernel<16, 16, 2, 2, 6>, 256, "256x2 flush16"},
+    {batch_field_kernel<16, 8, 4, 2, 6>, 128, "128x4 flush16"}};
+static const BatchKernel kAdjointFlush64Kernels[] = {   // accuracy/speed study
+    {batch_field_kernel<16, 16, 2, 2, 7>, 256, "256x2 flush64"},
+    {batch_field_kernel<16, 8, 4, 2, 7>, 128, "128x4 flush64"}};
+constexpr int kMaxCandidates = 12;
 
 #define VEXT_COUNT(t) (int)(sizeof t / sizeof t[0])
 
 // kind: 0 forward, 1 forward + adjoint (default: reciprocal of q, cubed),
-// 2 with the reciprocal of q^3 and a Newton step, 3 the same without it
+// 2 with the reciprocal of q^3 and a Newton step, 3 the same without it,
+// 4 / 5 default with FP32 gradient partials over 16 / 64 entries (a whole
+// 128-entry chunk by default; the energy partials always cover 16)
 static int batch_kernel_count(int kind) {
     switch (kind) {
     case 0: return VEXT_COUNT(kForwardKernels);
     case 1: return VEXT_COUNT(kAdjointKernels);
     case 2: return VEXT_COUNT(kAdjointNewtonKernels);
+    case 4: return VEXT_COUNT(kAdjointFlush16Kernels);
+    case 5: return VEXT_COUNT(kAdjointFlush64Kernels);
     default: return VEXT_COUNT(kAdjointRcp3Kernels);
     }
 }
@@ -390,6 +403,8 @@ static const BatchKernel &batch_kernel(int kind, int shape) {
     case 0: return kForwardKernels[shape];
     case 1: return kAdjointKernels[shape];
     case 2: return kAdjointNewtonKernels[shape];
+    case 4: return kAdjointFlush16Kernels[shape];
+    case 5: return kAdjointFlush64Kernels[shape];
     default: return kAdjointRcp3Kernels[shape];
     }
 }
@@ -490,7 +505,12 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
     b->n_axes = n_axes;
     b->opt = resolve_options(opt);
     b->adj = gradients != nullptr;
-    b->kind = !b->adj ? 0 : (b->opt.variant & 32) ? 2 : (b->opt.variant & 64) ? 3 : 1;
+    b->kind = !b->adj                 ? 0
+              : (b->opt.variant & 32)  ? 2
+              : (b->opt.variant & 64)  ? 3
+              : (b->opt.variant & 128) ? 4
+              : (b->opt.variant & 512) ? 5
+                                       : 1;
     if (b->opt.mode != VEXT_MODE_MIXED)
         return fail(VEXT_ERR_ARGUMENT, "batched fields run in the mixed mode only");
     int dev = 0;

@@ -438,8 +438,8 @@ __device__ __forceinline__ void near_chunk_adj(const double *ed, const double *s
 // MASK = false for inner entries (inside the cutoff of every site of every
 // pose of the region): no mask, and the shift, the same for every pose, is
 // summed once per entry into shift_sum (the caller adds 2 x shift_sum, both
-// sites, to every energy).  FP32 partials over FLUSH entries are flushed into
-// the FP64 AdjAcc.
+// sites, to every energy).  FP32 partials are flushed into the FP64 AdjAcc:
+// the energy every 16 entries, the gradient sums every FLUSH entries.
 template <int P, bool NEWTON, int FLUSH, bool MASK, bool RCP1 = true, int UNROLL = 1>
 __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *stf, int len,
                                               const FarGeom &g, const float2 (&ux)[P / 2],
@@ -450,21 +450,25 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
     const float2 one2 = make_float2(1.f, 1.f);
 #pragma unroll 1
     for (int e0 = 0; e0 < len; e0 += FLUSH) {
-        float2 fe[PP], fh[PP][2][3], ff[PP][2];
-        float fs = 0.f;
+        float2 fh[PP][2][3], ff[PP][2];
 #pragma unroll
-        for (int j = 0; j < PP; ++j) {
-            fe[j] = make_float2(0.f, 0.f);
+        for (int j = 0; j < PP; ++j)
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
                 ff[j][q] = make_float2(0.f, 0.f);
 #pragma unroll
                 for (int k = 0; k < 3; ++k) fh[j][q][k] = make_float2(0.f, 0.f);
             }
-        }
         const int e1 = min(e0 + FLUSH, len);
+#pragma unroll 1
+        for (int b0 = e0; b0 < e1; b0 += 16) {   // energy partials: 16 entries
+        float2 fe[PP];
+        float fs = 0.f;
+#pragma unroll
+        for (int j = 0; j < PP; ++j) fe[j] = make_float2(0.f, 0.f);
+        const int b1 = min(b0 + 16, e1);
 #pragma unroll UNROLL
-        for (int e = e0; e < e1; ++e) {
+        for (int e = b0; e < b1; ++e) {
             const float4 h = hb[e];
             const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, -)
             const float dx = h.x - g.cx, dy = h.y - g.cy, dz = h.z - g.cz;
@@ -533,9 +537,13 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
         if (!MASK) shift_sum += (double)fs;
 #pragma unroll
         for (int j = 0; j < PP; ++j) {
+            acc[2 * j].e += (double)fe[j].x;
+            acc[2 * j + 1].e += (double)fe[j].y;
+        }
+        }
+#pragma unroll
+        for (int j = 0; j < PP; ++j) {
             AdjAcc &a0 = acc[2 * j], &a1 = acc[2 * j + 1];
-            a0.e += (double)fe[j].x;
-            a1.e += (double)fe[j].y;
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
                 a0.f[q] += (double)ff[j][q].x;
