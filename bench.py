@@ -49,7 +49,7 @@ METRIC = "Vext pose evals/s at <=1e-4 K vs FP64, fwd+adjoint evals/s; % FP32 pea
 FAR_DRAM_BYTES_FULL_FIELD = 743_810_048 + 100_710_144
 # the same for one forward + adjoint batch_field_kernel launch on full_field,
 # from an ncu capture (--set full) of `bench.py --profile adjoint`.
-ADJ_DRAM_BYTES_FULL_FIELD = 424_774_656 + 353_256_704
+ADJ_DRAM_BYTES_FULL_FIELD = 421_518_080 + 354_799_616
 CPU_CENTERS_PER_CORE_S = 900.0   # reference driver throughput estimate used to size the sample
 
 
