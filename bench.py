@@ -433,6 +433,7 @@ def secondary_measurements(args, system, case, size, axes, poses, pairs, far_pai
                                "same framework", "flop_per_pair": FLOP_FWD_ADJ}
     del cart, q, e, gc, gq
     out["precision_study"] = precision_study(device)
+    out["string_update"] = bench_string_update()
     if not args.no_batch:
         out["batch"] = bench_batch(args, size, axes, device, stream, adjoint=False)
         out["batch_fwd_adjoint"] = bench_batch(args, size, axes, device, stream, adjoint=True)
@@ -472,6 +473,27 @@ def precision_study(device):
                 res[label] = stats
         out[name] = res
     return out
+
+
+def bench_string_update():
+    """The GPU String update on the config-4 path (small_field framework,
+    64 images along c from (0.25, 0.25, 0) to (0.25, 0.25, 1), seed-3
+    quaternions): 200 iterations with forces, step, end fixing,
+    reparametrisation, smoothing and the convergence test (vext_string_run)."""
+    from string_vext_b200 import synth
+    from string_vext_b200.string_path import euler_from_quaternions, run_string
+    from string_vext_b200.system import VextSystem
+    case, frac, quat, _, _ = synth.string_path()
+    path = np.column_stack([frac, np.mod(euler_from_quaternions(quat), 2 * np.pi)])
+    with VextSystem(case) as system:
+        run_string(system, path, direction=3, max_iterations=2)       # lists, scratch
+        t0 = time.perf_counter()
+        _, _, res = run_string(system, path, direction=3, max_iterations=200)
+        wall = time.perf_counter() - t0
+    return {"iterations": res["iterations"], "images": len(path), "seconds": wall,
+            "ms_per_iteration": 1e3 * wall / max(res["iterations"], 1),
+            "workload": "config-4 path, 64 images, 200 iterations, host wall time of "
+                        "vext_string_run (graph-replayed iterations)"}
 
 
 def bench_string_batch(device, stream):

@@ -58,6 +58,19 @@ struct RegionSet {
     ~RegionSet();
 };
 
+// One system's view for the warp-per-pose kernel (posebatch.cu).
+struct PoseBatchSys {
+    Mat3 H, Hinv;
+    double rc2;
+    float rc2f;
+    double off0, off1;
+    int nb0, nb1, nb2;
+    const RegionInfo *regs;
+    const float4 *hi, *lo;
+    const double *td;   // (c12, c6, shift, floor2) per type
+    const float4 *tf;
+};
+
 struct System {
     int device = 0;
     Mat3 H, Hinv;
@@ -92,6 +105,9 @@ struct System {
     size_t pose_scratch_cap = 0;
     double *d_pose_io = nullptr;     // host-pointer entry staging
     size_t pose_io_cap = 0;
+    PoseBatchSys *d_pose_desc = nullptr;   // warp-per-pose path: device copy of h_pose_desc
+    PoseBatchSys h_pose_desc;
+    long long *d_pose_offsets = nullptr;
     cudaStream_t stream = nullptr;   // private stream for host-pointer entries
     cudaStream_t aux = nullptr;      // second stream: near pairs beside far pairs
     cudaEvent_t fork = nullptr, join = nullptr;
@@ -163,6 +179,12 @@ int pose_enqueue(System *sys, int n, const double *centers, const double *quats,
                  const Options &o, double *energy, double *gc, double *gq, double *gu,
                  cudaStream_t st);
 int pose_status(System *sys, cudaStream_t st);
+
+// Warp-per-pose evaluation of n poses of one system on its bin lists `rs`
+// (small batches, where the binned pipeline's per-bin CTAs would idle).
+int pose_warp_enqueue(System *sys, const RegionSet *rs, int n, const double *centers,
+                      const double *quats, const Options &o, double *energy, double *gc,
+                      double *gq, double *gu, cudaStream_t st);
 
 // Field kernel launcher (field.cu): computes E64 [O][S^3] for all regions.
 int launch_field(System *sys, const RegionSet *rs, int n_axes, const double *d_axes,

@@ -420,6 +420,12 @@ int pose_enqueue(System *sys, int n, const double *centers, const double *quats,
     RegionSet *rs = nullptr;
     VEXT_TRY(get_bin_regions(sys, r_split, &rs, st));
     const int n_bins = rs->n_regions;
+    // Fewer than 64 poses per bin on average: the binned pipeline would give
+    // most of its per-bin CTAs a handful of poses for a whole list each; one
+    // warp per pose is faster there (String paths, small batches).
+    if ((long long)n < 64LL * n_bins)
+        return pose_warp_enqueue(sys, rs, n, centers, quats, o,
+                                 energy ? energy : nullptr, gc, gq, gu, st);
     const int max_items = n_bins + (n + kPoseThreads - 1) / kPoseThreads;
     const size_t bytes = pose_scratch_bytes(n, n_bins, max_items, false);
     VEXT_TRY(ensure_capacity(*reinterpret_cast<char **>(&sys->d_pose_scratch),

@@ -13,24 +13,13 @@
 // dE/du.  Pair term and forces as in pose.cu.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <memory>
 #include <vector>
 
 #include "internal.cuh"
 
 namespace vext {
-
-struct PoseBatchSys {
-    Mat3 H, Hinv;
-    double rc2;
-    float rc2f;
-    double off0, off1;
-    int nb0, nb1, nb2;
-    const RegionInfo *regs;
-    const float4 *hi, *lo;
-    const double *td;   // (c12, c6, shift, floor2) per type
-    const float4 *tf;
-};
 
 struct PoseBatchArgs {
     const PoseBatchSys *sys;
@@ -197,6 +186,66 @@ __global__ void __launch_bounds__(256) pose_batch_kernel(PoseBatchArgs a) {
     }
 }
 
+static PoseBatchSys describe(const System *sys, const RegionSet *rs) {
+    PoseBatchSys y;
+    std::memset(&y, 0, sizeof y);   // padding too: descriptors are compared bytewise
+    y.H = sys->H;
+    y.Hinv = sys->Hinv;
+    y.rc2 = sys->cutoff * sys->cutoff;
+    y.rc2f = (float)y.rc2;
+    y.off0 = sys->offsets[0];
+    y.off1 = sys->offsets[1];
+    y.nb0 = rs->nb[0];
+    y.nb1 = rs->nb[1];
+    y.nb2 = rs->nb[2];
+    y.regs = rs->d_info;
+    y.hi = rs->d_hi;
+    y.lo = rs->d_lo;
+    y.td = sys->d_td;
+    y.tf = sys->d_tf;
+    return y;
+}
+
+int pose_warp_enqueue(System *sys, const RegionSet *rs, int n, const double *centers,
+                      const double *quats, const Options &o, double *energy, double *gc,
+                      double *gq, double *gu, cudaStream_t st) {
+    // The descriptor is uploaded synchronously on first use and whenever the
+    // bin lists moved (compared with the host copy of the last upload); inside
+    // a stream capture it is therefore already in place.
+    const PoseBatchSys y = describe(sys, rs);
+    const bool upload =
+        !sys->d_pose_desc || std::memcmp(&sys->h_pose_desc, &y, sizeof y) != 0;
+    if (!sys->d_pose_desc) {
+        VEXT_CUDA(cudaMalloc(&sys->d_pose_desc, sizeof(PoseBatchSys)));
+        VEXT_CUDA(cudaMalloc(&sys->d_pose_offsets, 2 * sizeof(long long)));
+        const long long off[2] = {0, 0};   // one system: the kernel never reads them
+        VEXT_CUDA(cudaMemcpy(sys->d_pose_offsets, off, sizeof off, cudaMemcpyHostToDevice));
+    }
+    if (upload) {
+        VEXT_CUDA(cudaMemcpy(sys->d_pose_desc, &y, sizeof y, cudaMemcpyHostToDevice));
+        std::memcpy(&sys->h_pose_desc, &y, sizeof y);
+    }
+    PoseBatchArgs a;
+    a.sys = sys->d_pose_desc;
+    a.offsets = sys->d_pose_offsets;
+    a.n_systems = 1;
+    a.n = n;
+    a.centers = centers;
+    a.quats = quats;
+    a.energy = energy;
+    a.gc = gc;
+    a.gq = gq;
+    a.gu = gu;
+    const bool band = o.mode == VEXT_MODE_MIXED && o.band_hi > o.band_lo;
+    a.band_lo = band ? o.band_lo : 0.0;
+    a.band_hi = band ? o.band_hi : 0.0;
+    a.status = sys->d_status;
+    const long long blocks = std::min<long long>(((long long)n + 7) / 8, 148LL * 16);
+    pose_batch_kernel<<<(int)blocks, 256, 0, st>>>(a);
+    VEXT_CUDA(cudaGetLastError());
+    return 0;
+}
+
 }  // namespace vext
 
 using namespace vext;
@@ -247,21 +296,7 @@ extern "C" int vext_pose_batch_create(int n_systems, const vext_system *systems,
         std::lock_guard<std::mutex> lock(sys->lock);
         RegionSet *rs = nullptr;
         VEXT_TRY(get_bin_regions(sys, r_split, &rs, sys->stream));
-        PoseBatchSys &y = hs[k];
-        y.H = sys->H;
-        y.Hinv = sys->Hinv;
-        y.rc2 = sys->cutoff * sys->cutoff;
-        y.rc2f = (float)y.rc2;
-        y.off0 = sys->offsets[0];
-        y.off1 = sys->offsets[1];
-        y.nb0 = rs->nb[0];
-        y.nb1 = rs->nb[1];
-        y.nb2 = rs->nb[2];
-        y.regs = rs->d_info;
-        y.hi = rs->d_hi;
-        y.lo = rs->d_lo;
-        y.td = sys->d_td;
-        y.tf = sys->d_tf;
+        hs[k] = describe(sys, rs);
     }
     std::vector<long long> offs(pose_offsets, pose_offsets + n_systems + 1);
     VEXT_CUDA(cudaMalloc(&b->d_sys, sizeof(PoseBatchSys) * n_systems));

@@ -449,6 +449,8 @@ System::~System() {
     cudaFree(d_flags);
     cudaFree(d_pose_scratch);
     cudaFree(d_pose_io);
+    cudaFree(d_pose_desc);
+    cudaFree(d_pose_offsets);
     for (auto &e : ev)
         if (e) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
