@@ -204,6 +204,21 @@ def error_stats(mixed, exact):
             "passed": bool((diff[neg] < 1e-4).all() and (rel[~neg] < 1e-6).all())}
 
 
+def hbm_check(traffic_bytes, ms):
+    """The kernel's DRAM throughput (ncu bytes / device time) against the
+    measured HBM copy bandwidth in MEASURED_PEAKS.json."""
+    try:
+        peak = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]
+        source = "MEASURED_PEAKS.json hbm_gbs"
+    except (OSError, KeyError, ValueError):
+        peak, source = 6650.0, "fallback 6.65 TB/s"
+    if not traffic_bytes:
+        return {"achieved": None, "peak": peak, "unit": "GB/s", "peak_source": source}
+    achieved = traffic_bytes / (ms * 1e-3) / 1e9
+    return {"achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": source}
+
+
 def timed_region(fn, steps, stream):
     """CUDA-event time (ms) of `steps` calls of fn on `stream`."""
     import torch
@@ -319,6 +334,12 @@ def run_ours(args, rank, world, local_rank):
                          "traffic": (ADJ_DRAM_BYTES_FULL_FIELD
                                      if args.workload == "full_field" else None),
                          "traffic_unit": "bytes per launch (ncu dram__bytes_read+write)",
+                         "bound_note": "non-tensor FP32 SIMT pipe: pairwise LJ is not a dense "
+                                       "contraction, so neither the HBM nor the tensor-core "
+                                       "roofline applies; see hbm_check",
+                         "hbm_check": hbm_check(ADJ_DRAM_BYTES_FULL_FIELD
+                                                if args.workload == "full_field" else None,
+                                                ms_step),
                          "pipes": pipes},
             "clocks": clocks.summary(), "cpu_baseline": cpu}
     line.update(extra)
