@@ -205,7 +205,9 @@ VEXT_API int vext_field_adjoint_device(vext_system sys, int size, int n_axes,
                                        float *energy, float *gradient, double *energy_f64,
                                        double *gradient_f64, void *stream);
 /* Same with HOST float32 outputs (staged on the device, copied back before
- * the call returns). */
+ * the call returns).  In the mixed mode with more than 32 directors the poses
+ * run as one batch per 32-director block and each block's outputs are copied
+ * back while the next block computes. */
 VEXT_API int vext_field_adjoint(vext_system sys, int size, int n_axes, const double *axes,
                                 const vext_options *opt, float *energy, float *gradient);
 

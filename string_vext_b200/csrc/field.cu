@@ -948,6 +948,58 @@ extern "C" int vext_field_adjoint(vext_system h, int size, int n_axes, const dou
     VEXT_TRY(ensure_capacity(sys->d_f32, sys->f32_cap, n));
     VEXT_TRY(ensure_capacity(sys->d_g32, sys->g32_cap, 6 * n));
     cudaStream_t st = sys->stream;
+    if (o.mode == VEXT_MODE_MIXED && n_axes > 32) {
+        // one batch per 32-director block; block k's copy (on aux) overlaps
+        // block k + 1's pair work (on st)
+        for (int k = 0; k < 3 * n_axes; ++k)
+            if (!std::isfinite(axes[k])) return fail(VEXT_ERR_ARGUMENT, "non-finite director");
+        const size_t S3 = (size_t)size * size * size;
+        const int parts = (n_axes + 31) / 32;
+        const bool same = (int)sys->host_parts.size() == parts && sys->host_size == size &&
+                          sys->host_axes.size() == 3 * (size_t)n_axes &&
+                          std::equal(axes, axes + 3 * n_axes, sys->host_axes.begin()) &&
+                          sys->host_key[0] == o.r_split && sys->host_key[1] == o.band_lo &&
+                          sys->host_key[2] == o.band_hi && sys->host_key[3] == o.variant &&
+                          sys->host_e == sys->d_f32 && sys->host_g == sys->d_g32;
+        if (!same) {
+            sys->drop_host_parts();
+            for (int k = 0; k < parts; ++k) {
+                const int nk = std::min(32, n_axes - 32 * k);
+                float *ek = sys->d_f32 + 32 * (size_t)k * S3;
+                float *gk = sys->d_g32 + 6 * 32 * (size_t)k * S3;
+                vext_batch b = nullptr;
+                VEXT_TRY(batch_build(1, &h, size, nk, axes + 3 * 32 * k, opt, &ek, &gk, nullptr,
+                                     false, &b));
+                sys->host_parts.push_back(b);
+                cudaEvent_t ev;
+                VEXT_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+                sys->host_part_done.push_back(ev);
+            }
+            sys->host_size = size;
+            sys->host_axes.assign(axes, axes + 3 * n_axes);
+            sys->host_key[0] = o.r_split;
+            sys->host_key[1] = o.band_lo;
+            sys->host_key[2] = o.band_hi;
+            sys->host_key[3] = o.variant;
+            sys->host_e = sys->d_f32;
+            sys->host_g = sys->d_g32;
+        }
+        for (int k = 0; k < parts; ++k) {
+            const size_t first = 32 * (size_t)k * S3, count = std::min(32, n_axes - 32 * k) * S3;
+            VEXT_TRY(batch_replay(sys->host_parts[k], st));
+            VEXT_CUDA(cudaEventRecord(sys->host_part_done[k], st));
+            VEXT_CUDA(cudaStreamWaitEvent(sys->aux, sys->host_part_done[k], 0));
+            VEXT_CUDA(cudaMemcpyAsync(energy + first, sys->d_f32 + first, sizeof(float) * count,
+                                      cudaMemcpyDeviceToHost, sys->aux));
+            VEXT_CUDA(cudaMemcpyAsync(gradient + 6 * first, sys->d_g32 + 6 * first,
+                                      sizeof(float) * 6 * count, cudaMemcpyDeviceToHost,
+                                      sys->aux));
+        }
+        VEXT_CUDA(cudaStreamSynchronize(sys->aux));
+        VEXT_CUDA(cudaStreamSynchronize(st));
+        for (vext_batch b : sys->host_parts) VEXT_TRY(vext_batch_status(b));
+        return 0;
+    }
     VEXT_TRY(field_adjoint_device(h, size, n_axes, axes, o, opt, sys->d_f32, sys->d_g32, nullptr,
                                   nullptr, st));
     VEXT_CUDA(cudaMemcpyAsync(energy, sys->d_f32, sizeof(float) * n, cudaMemcpyDeviceToHost, st));

@@ -127,8 +127,18 @@ struct System {
     double *adj_energy64 = nullptr;
     float *d_g32 = nullptr;          // host-output staging of the float32 gradient
     size_t g32_cap = 0;
+    // the host entry's batches (vext_field_adjoint): one per 32-director
+    // block, each writing its contiguous slice of d_f32 / d_g32, so the copy
+    // of one block overlaps the next block's pair work
+    std::vector<vext_batch> host_parts;
+    std::vector<cudaEvent_t> host_part_done;
+    int host_size = 0;
+    std::vector<double> host_axes;
+    double host_key[4] = {0, 0, 0, 0};
+    float *host_e = nullptr, *host_g = nullptr;
     std::mutex lock;
-    void drop_adjoint_batch();
+    void drop_adjoint_batch();   // both caches (they point into the region sets)
+    void drop_host_parts();
     ~System();
 };
 

@@ -429,6 +429,16 @@ void System::drop_adjoint_batch() {
     adj_batch = nullptr;
     adj_size = 0;
     adj_axes.clear();
+    drop_host_parts();
+}
+
+void System::drop_host_parts() {
+    for (vext_batch b : host_parts) vext_batch_destroy(b);
+    for (cudaEvent_t e : host_part_done) cudaEventDestroy(e);
+    host_parts.clear();
+    host_part_done.clear();
+    host_size = 0;
+    host_axes.clear();
 }
 
 System::~System() {
