@@ -62,16 +62,62 @@ struct BatchArgs {
 // (pair.cuh); writes the energy and [dE/dc, tangent dE/du] of every pose.
 // Far entries come in two passes: inner (no cutoff mask, shift summed once
 // per entry) and shell.
-template <int CB, int G, int P, bool NEWTON, bool RCP1, int UNROLL, int FLUSH>
+// GSUM: the FP64 gradient sums wait in shared memory (gsum) during the far
+// passes, so those passes hold only the energy sums and FP32 partials.
+template <int CB, int G, int P, bool NEWTON, bool RCP1, int UNROLL, int FLUSH, bool GSUM>
 __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSys &y,
                                                const RegionInfo &r, Stager &st, double *ed,
                                                const float4 *stf, const double *std4,
-                                               unsigned &seq, double cx, double cy, double cz,
-                                               int obase, double (&e)[P], double (&gr)[P][6]) {
+                                               double *gsum, unsigned &seq, double cx,
+                                               double cy, double cz, int obase, double (&e)[P],
+                                               double (&gr)[P][6]) {
     constexpr int NT = CB * G, PP = P / 2;
     AdjAcc acc[P];
     adj_zero(acc);
-    {
+    if constexpr (GSUM) {
+        static_assert(PP <= 2, "two director pairs at most");
+        // near pairs two directors at a time (the near list is staged once
+        // per pair): the FP64 sums of two directors in registers, their
+        // gradient parts parked in gsum, the energies kept in acc
+        const NearGeom g = near_geom(cx, cy, cz, y.off0, y.off1, y.rc2);
+#pragma unroll 1
+        for (int half = 0; half < PP; ++half) {
+            AdjAcc a2[2];
+            adj_zero(a2);
+            double ux[2], uy[2], uz[2];
+#pragma unroll
+            for (int p = 0; p < 2; ++p) {
+                const int o = min(obase + G * (2 * half + p), y.O - 1);
+                ux[p] = y.axes[3 * o];
+                uy[p] = y.axes[3 * o + 1];
+                uz[p] = y.axes[3 * o + 2];
+            }
+            ChunkPlan plan;
+            plan.init_range(r.off, r.n_near, r.n_near);
+            stage_prologue(st, plan, y.hi, y.lo, seq);
+            for (int c = 0; c < plan.n_chunks; ++c) {
+                if (!stage_wait(st, plan, c, seq, a.status)) return false;
+                int start, len;
+                bool near;
+                plan.chunk(c, start, len, near);
+                const int s = (seq + c) % kStages;
+                near_convert<NT>(st.hib + s * kCH, st.lob + s * kCH, ed, len);
+                __syncthreads();
+                if (y.near_mode == 2) near_chunk_adj<2, 2>(ed, std4, len, g, ux, uy, uz, a2);
+                else near_chunk_adj<2, 1>(ed, std4, len, g, ux, uy, uz, a2);
+                stage_next(st, plan, y.hi, y.lo, c, seq);
+            }
+            seq += plan.n_chunks;
+            grad_store<NT>(gsum, a2, 2 * half);
+            if (half == 0) {
+                acc[0].e = a2[0].e;
+                acc[1].e = a2[1].e;
+            } else {
+                acc[2 * PP - 2].e = a2[0].e;
+                acc[2 * PP - 1].e = a2[1].e;
+            }
+        }
+    } else {
         double ux[P], uy[P], uz[P];
 #pragma unroll
         for (int p = 0; p < P; ++p) {
@@ -122,17 +168,19 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
                 bool near;
                 plan.chunk(c, start, len, near);
                 const float4 *hb = st.hib + ((seq + c) % kStages) * kCH;
+                constexpr int GNT = GSUM ? NT : 0;
                 if (pass)
-                    far_chunk_adj<P, NEWTON, FLUSH, true, RCP1, UNROLL>(hb, stf, len, g, ux, uy,
-                                                                        uz, acc, shift_sum);
+                    far_chunk_adj<P, NEWTON, FLUSH, true, RCP1, UNROLL, GNT>(
+                        hb, stf, len, g, ux, uy, uz, acc, shift_sum, gsum);
                 else
-                    far_chunk_adj<P, NEWTON, FLUSH, false, RCP1, UNROLL>(hb, stf, len, g, ux, uy,
-                                                                         uz, acc, shift_sum);
+                    far_chunk_adj<P, NEWTON, FLUSH, false, RCP1, UNROLL, GNT>(
+                        hb, stf, len, g, ux, uy, uz, acc, shift_sum, gsum);
                 stage_next(st, plan, y.hi, y.lo, c, seq);
             }
             seq += plan.n_chunks;
         }
     }
+    if constexpr (GSUM) grad_load<NT>(gsum, acc);
 #pragma unroll
     for (int p = 0; p < P; ++p) {
         const int o = min(obase + G * p, y.O - 1);
@@ -147,7 +195,8 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
 // 1 = rcp(q) cubed (default), 2 = rcp(q^3) + Newton, 3 = rcp(q^3);
 // 5 = as 1 with the far entry loop unrolled twice; 6 / 7 = as 1 with the
 // FP32 gradient partials flushed every 16 / 64 entries instead of once per
-// 128-entry chunk.
+// 128-entry chunk; 8 = as 1 with the FP64 gradient sums in shared memory
+// during the far passes (fewer registers: more resident CTAs).
 template <int CB, int G, int P, int MINB, int ADJ>
 __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
     constexpr int NT = CB * G, PP = P / 2;
@@ -189,9 +238,11 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
         double e[P];
         double gr[ADJ ? P : 1][6];
         if constexpr (ADJ) {
+            double *gsum = reinterpret_cast<double *>(std4 + 4 * y.n_types);
             if (!batch_item_adj<CB, G, P, ADJ == 2, ADJ == 1 || ADJ >= 5,
-                                ADJ == 5 ? 2 : 1, ADJ == 6 ? 16 : ADJ == 7 ? 64 : 128>(
-                    a, y, r, st, ed, stf, std4, seq, cx, cy, cz, obase, e, gr))
+                                ADJ == 5 ? 2 : 1, ADJ == 6 ? 16 : ADJ == 7 ? 64 : 128,
+                                ADJ == 8>(a, y, r, st, ed, stf, std4, gsum, seq, cx, cy, cz,
+                                          obase, e, gr))
                 return;
         } else {
         // ---- near pairs (FP64)
@@ -366,7 +417,8 @@ static const BatchKernel kAdjointKernels[] = {
     {batch_field_kernel<16, 16, 2, 2, 1>, 256, "256x2"},
     {batch_field_kernel<16, 8, 4, 2, 1>, 128, "128x4"},
     {batch_field_kernel<16, 8, 4, 3, 1>, 128, "128x4/3"},
-    {batch_field_kernel<16, 16, 2, 2, 5>, 256, "256x2 unroll2"}};
+    {batch_field_kernel<16, 16, 2, 2, 5>, 256, "256x2 unroll2"},
+    {batch_field_kernel<16, 8, 4, 3, 8>, 128, "128x4/3 gsum"}};
 static const BatchKernel kAdjointNewtonKernels[] = {   // accuracy/speed study
     {batch_field_kernel<16, 16, 2, 2, 2>, 256, "256x2 rcp3+newton"},
     {batch_field_kernel<16, 8, 4, 2, 2>, 128, "128x4 rcp3+newton"}};
@@ -449,8 +501,11 @@ struct vext_batch_s {
     }
 };
 
-static size_t batch_smem(int max_types) {
-    return kStageBytes + (size_t)kCH * 4 * sizeof(double) + (size_t)max_types * 48;
+// Staging + converted near chunk + type tables (+ the FP64 gradient sums of
+// 16 centers x 32 directors for the adjoint kernels that park them there).
+static size_t batch_smem(int max_types, bool adj) {
+    return kStageBytes + (size_t)kCH * 4 * sizeof(double) + (size_t)max_types * 48 +
+           (adj ? (size_t)kGradWords * 16 * 32 * sizeof(double) : 0);
 }
 
 static int batch_launch(vext_batch b, const BatchConfig &cfg, const int4 *items, int n_items,
@@ -465,7 +520,7 @@ static int batch_launch(vext_batch b, const BatchConfig &cfg, const int4 *items,
     a.band_lo = b->opt.band_lo;
     a.band_hi = b->opt.band_hi;
     a.status = b->d_status;
-    const size_t smem = batch_smem(b->max_types);
+    const size_t smem = batch_smem(b->max_types, b->adj);
     VEXT_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(int), st));
     VEXT_CUDA(cudaMemsetAsync(b->d_refine, 0, sizeof(int), st));
     const BatchKernel &k = batch_kernel(b->kind, cfg.shape);
@@ -585,7 +640,7 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
     VEXT_CUDA(cudaMalloc(&b->d_status, sizeof(int)));
     VEXT_CUDA(cudaMemset(b->d_status, 0, sizeof(int)));
     // ---- autotune: CTA shape x resident CTAs per SM, on the sampled queue
-    const size_t smem = batch_smem(b->max_types);
+    const size_t smem = batch_smem(b->max_types, b->adj);
     int sms = 0;
     VEXT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     // candidates: every kernel of the mode at its full and at half its occupancy

@@ -429,6 +429,43 @@ __device__ __forceinline__ void near_chunk_adj(const double *ed, const double *s
     }
 }
 
+// Shared-memory home of the FP64 gradient sums (H_s, F_s) of a CTA for
+// kernels that keep only the energy sums in registers during the far passes:
+// component k (0-2 = h[0], 3-5 = h[1], 6-7 = f) of director p of thread t is
+// gsum[(p * kGradWords + k) * NT + t] (consecutive threads, consecutive words).
+constexpr int kGradWords = 8;
+
+template <int NT>
+__device__ __forceinline__ double &grad_slot(double *gsum, int p, int k) {
+    return gsum[(p * kGradWords + k) * NT + threadIdx.x];
+}
+
+// Directors p0 .. p0 + P - 1 of the shared-memory sums from acc.
+template <int NT, int P>
+__device__ __forceinline__ void grad_store(double *gsum, const AdjAcc (&acc)[P], int p0 = 0) {
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                grad_slot<NT>(gsum, p0 + p, 3 * q + k) = acc[p].h[q][k];
+            grad_slot<NT>(gsum, p0 + p, 6 + q) = acc[p].f[q];
+        }
+}
+
+template <int NT, int P>
+__device__ __forceinline__ void grad_load(double *gsum, AdjAcc (&acc)[P]) {
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) acc[p].h[q][k] = grad_slot<NT>(gsum, p, 3 * q + k);
+            acc[p].f[q] = grad_slot<NT>(gsum, p, 6 + q);
+        }
+}
+
 // Packed FP32x2 far chunk, forward + adjoint (lanes = two directors).  Per
 // site, by default (RCP1): n1 = hardware reciprocal of q per lane, n3 = n1^3 =
 // q^-3, e = n3 (c12 n3 - c6) + m shift, fp = (n1 n3) (c6 - 2 c12 n3) =
@@ -440,12 +477,15 @@ __device__ __forceinline__ void near_chunk_adj(const double *ed, const double *s
 // summed once per entry into shift_sum (the caller adds 2 x shift_sum, both
 // sites, to every energy).  FP32 partials are flushed into the FP64 AdjAcc:
 // the energy every 16 entries, the gradient sums every FLUSH entries.
-template <int P, bool NEWTON, int FLUSH, bool MASK, bool RCP1 = true, int UNROLL = 1>
+// GSUM_NT > 0: the gradient partials go to the shared-memory sums
+// (grad_slot<GSUM_NT>(gsum, ...)) instead of acc (whose energies stay).
+template <int P, bool NEWTON, int FLUSH, bool MASK, bool RCP1 = true, int UNROLL = 1,
+          int GSUM_NT = 0>
 __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *stf, int len,
                                               const FarGeom &g, const float2 (&ux)[P / 2],
                                               const float2 (&uy)[P / 2],
                                               const float2 (&uz)[P / 2], AdjAcc (&acc)[P],
-                                              double &shift_sum) {
+                                              double &shift_sum, double *gsum = nullptr) {
     constexpr int PP = P / 2;
     const float2 one2 = make_float2(1.f, 1.f);
 #pragma unroll 1
@@ -541,17 +581,33 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
             acc[2 * j + 1].e += (double)fe[j].y;
         }
         }
+        if constexpr (GSUM_NT > 0) {
 #pragma unroll
-        for (int j = 0; j < PP; ++j) {
-            AdjAcc &a0 = acc[2 * j], &a1 = acc[2 * j + 1];
+            for (int j = 0; j < PP; ++j)
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                a0.f[q] += (double)ff[j][q].x;
-                a1.f[q] += (double)ff[j][q].y;
+                for (int l = 0; l < 2; ++l)
 #pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    a0.h[q][k] += (double)fh[j][q][k].x;
-                    a1.h[q][k] += (double)fh[j][q][k].y;
+                    for (int q = 0; q < 2; ++q) {
+#pragma unroll
+                        for (int k = 0; k < 3; ++k)
+                            grad_slot<GSUM_NT>(gsum, 2 * j + l, 3 * q + k) +=
+                                (double)(l ? fh[j][q][k].y : fh[j][q][k].x);
+                        grad_slot<GSUM_NT>(gsum, 2 * j + l, 6 + q) +=
+                            (double)(l ? ff[j][q].y : ff[j][q].x);
+                    }
+        } else {
+#pragma unroll
+            for (int j = 0; j < PP; ++j) {
+                AdjAcc &a0 = acc[2 * j], &a1 = acc[2 * j + 1];
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    a0.f[q] += (double)ff[j][q].x;
+                    a1.f[q] += (double)ff[j][q].y;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        a0.h[q][k] += (double)fh[j][q][k].x;
+                        a1.h[q][k] += (double)fh[j][q][k].y;
+                    }
                 }
             }
         }
