@@ -49,7 +49,7 @@ METRIC = "Vext pose evals/s at <=1e-4 K vs FP64, fwd+adjoint evals/s; % FP32 pea
 FAR_DRAM_BYTES_FULL_FIELD = 743_810_048 + 100_710_144
 # the same for one forward + adjoint batch_field_kernel launch on full_field,
 # from an ncu capture (--set full) of `bench.py --profile adjoint`.
-ADJ_DRAM_BYTES_FULL_FIELD = 421_518_080 + 354_799_616
+ADJ_DRAM_BYTES_FULL_FIELD = 423_897_344 + 352_798_720
 CPU_CENTERS_PER_CORE_S = 900.0   # reference driver throughput estimate used to size the sample
 
 
@@ -323,7 +323,7 @@ def run_ours(args, rank, world, local_rank):
             "gpu_launches": args.steps * 2,
             "setup_s": setup_s,
             "roofline": {"bound": "fp32",
-                         "kernel": "batch_field_kernel<adjoint> (fused FP64 near + FP32x2 far)",
+                         "kernel": "batch_field_kernel<adjoint> (fused FP64 near + FP32x2 far, autotuned shape)",
                          "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
                          "frac": achieved / peak,
                          "peak_source": "measured on this GPU: max(FFMA, FFMA2) FMA rate x 2 "
