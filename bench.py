@@ -162,6 +162,33 @@ def cpu_reference_sample(case, size, n_axes, seconds_target, processes):
             "seconds": compute, "poses": poses}
 
 
+def cpu_reference_single_core(case, size, n_axes, seconds_target):
+    """The reference CPU path in its own mode (one process, one thread): the
+    reference driver in this process on a strided sample of the grid
+    centers; poses/s with and without the kd-tree query."""
+    from oracle import oracle
+    from string_vext_b200.orientation import regular_pose_grid
+    library, kind, symbol = oracle.REF_KERNEL, "reference", "evaluate_reused_neighbors"
+    if not library.exists():
+        library, kind, symbol = oracle.LIB_PATH, "port", "oracle_reused_neighbors"
+    centers, axes = regular_pose_grid(size, n_axes)
+    n_sample = int(min(len(centers), max(512, CPU_CENTERS_PER_CORE_S * seconds_target)))
+    stride = max(1, len(centers) // n_sample)
+    sample = centers[::stride][:n_sample]
+    driver = oracle.ReferenceDriver(case, library, symbol=symbol)
+    t0 = time.perf_counter()
+    driver.evaluate(sample, axes)
+    wall = time.perf_counter() - t0
+    poses = len(sample) * n_axes
+    return {"value": poses / wall, "unit": "poses/s", "cores": 1, "kind": kind,
+            "kernel_only": poses / driver.compute_seconds,
+            "query_share": driver.query_seconds / wall,
+            "sample": f"{len(sample)} of {len(centers)} grid centers (stride {stride}) x "
+                      f"{n_axes} directors, one process; {wall:.2f} s, kd-tree query "
+                      f"{driver.query_seconds:.2f} s, kernel {driver.compute_seconds:.2f} s, "
+                      f"{cpu_model()}"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -309,6 +336,7 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_cpu:
         cpu = cpu_reference_sample(case, size, n_axes, args.cpu_seconds, host_cores())
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        extra["cpu_baseline_single_core"] = cpu_reference_single_core(case, size, n_axes, 5.0)
     line = {"metric": METRIC, "value": value, "unit": "poses/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
