@@ -144,7 +144,10 @@ typedef struct {
                                 vext_default_options                          */
     int centers_per_region;  /* 16 or 32; 0 = default (16)                    */
     int variant;             /* pair-kernel shape; 0 = default                */
-    int reserved[3];
+    int batch_shape;         /* batches: 1 + index of the CTA shape to run at
+                                full occupancy instead of autotuning; 0 =
+                                autotune (vext_batch_tuning lists the shapes) */
+    int reserved[2];
 } vext_options;
 
 VEXT_API void vext_default_options(vext_options *opt);

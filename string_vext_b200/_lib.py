@@ -38,7 +38,7 @@ class Options(ctypes.Structure):
     _fields_ = [("mode", ctypes.c_int), ("r_split", ctypes.c_double),
                 ("band_lo", ctypes.c_double), ("band_hi", ctypes.c_double),
                 ("centers_per_region", ctypes.c_int), ("variant", ctypes.c_int),
-                ("reserved", ctypes.c_int * 3)]
+                ("batch_shape", ctypes.c_int), ("reserved", ctypes.c_int * 2)]
 
 
 class FieldStats(ctypes.Structure):
@@ -191,7 +191,8 @@ def ptr(array) -> ctypes.c_void_p | None:
 
 def options(mode: int = VEXT_MODE_MIXED, r_split: float | None = None,
             band: tuple[float, float] | None = None,
-            centers_per_region: int | None = None, variant: int | None = None) -> Options:
+            centers_per_region: int | None = None, variant: int | None = None,
+            batch_shape: int | None = None) -> Options:
     opt = Options()
     load().vext_default_options(ctypes.byref(opt))
     opt.mode = mode
@@ -203,6 +204,8 @@ def options(mode: int = VEXT_MODE_MIXED, r_split: float | None = None,
         opt.centers_per_region = centers_per_region
     if variant is not None:
         opt.variant = variant
+    if batch_shape is not None:
+        opt.batch_shape = batch_shape
     return opt
 
 

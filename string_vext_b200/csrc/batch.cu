@@ -646,7 +646,12 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
     // candidates: every kernel of the mode at its full and at half its occupancy
     BatchConfig cands[kMaxCandidates];
     int n_cands = 0;
-    for (int k = 0; k < batch_kernel_count(b->kind); ++k) {
+    const int n_kernels = batch_kernel_count(b->kind);
+    if (b->opt.batch_shape < 0 || b->opt.batch_shape > n_kernels)
+        return fail(VEXT_ERR_ARGUMENT, "batch_shape %d outside 0..%d", b->opt.batch_shape,
+                    n_kernels);
+    for (int k = 0; k < n_kernels; ++k) {
+        if (b->opt.batch_shape && k != b->opt.batch_shape - 1) continue;   // pinned shape
         const BatchKernel &bk = batch_kernel(b->kind, k);
         VEXT_CUDA(cudaFuncSetAttribute(bk.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
@@ -654,7 +659,8 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
         VEXT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bk.fn, bk.threads, smem));
         if (occ < 1) continue;
         if (n_cands < kMaxCandidates) cands[n_cands++] = {k, sms * occ};
-        if (occ >= 2 && n_cands < kMaxCandidates) cands[n_cands++] = {k, sms * (occ / 2)};
+        if (occ >= 2 && n_cands < kMaxCandidates && !b->opt.batch_shape)
+            cands[n_cands++] = {k, sms * (occ / 2)};
     }
     if (n_cands == 0) return fail(VEXT_ERR_CAPACITY, "batch kernel does not fit an SM");
     b->n_cands = n_cands;

@@ -885,7 +885,8 @@ static int field_adjoint_device(vext_system h, int size, int n_axes, const doubl
                           sys->adj_axes.size() == 3 * (size_t)n_axes &&
                           std::equal(axes, axes + 3 * n_axes, sys->adj_axes.begin()) &&
                           sys->adj_key[0] == o.r_split && sys->adj_key[1] == o.band_lo &&
-                          sys->adj_key[2] == o.band_hi && sys->adj_key[3] == o.variant &&
+                          sys->adj_key[2] == o.band_hi &&
+                          sys->adj_key[3] == o.variant + 65536.0 * o.batch_shape &&
                           sys->adj_energy == energy &&
                           sys->adj_grad == gradient && sys->adj_energy64 == energy_f64;
         if (!same) {
@@ -899,7 +900,7 @@ static int field_adjoint_device(vext_system h, int size, int n_axes, const doubl
             sys->adj_key[0] = o.r_split;
             sys->adj_key[1] = o.band_lo;
             sys->adj_key[2] = o.band_hi;
-            sys->adj_key[3] = o.variant;
+            sys->adj_key[3] = o.variant + 65536.0 * o.batch_shape;
             sys->adj_energy = energy;
             sys->adj_grad = gradient;
             sys->adj_energy64 = energy_f64;
@@ -959,7 +960,8 @@ extern "C" int vext_field_adjoint(vext_system h, int size, int n_axes, const dou
                           sys->host_axes.size() == 3 * (size_t)n_axes &&
                           std::equal(axes, axes + 3 * n_axes, sys->host_axes.begin()) &&
                           sys->host_key[0] == o.r_split && sys->host_key[1] == o.band_lo &&
-                          sys->host_key[2] == o.band_hi && sys->host_key[3] == o.variant &&
+                          sys->host_key[2] == o.band_hi &&
+                          sys->host_key[3] == o.variant + 65536.0 * o.batch_shape &&
                           sys->host_e == sys->d_f32 && sys->host_g == sys->d_g32;
         if (!same) {
             sys->drop_host_parts();
@@ -980,7 +982,7 @@ extern "C" int vext_field_adjoint(vext_system h, int size, int n_axes, const dou
             sys->host_key[0] = o.r_split;
             sys->host_key[1] = o.band_lo;
             sys->host_key[2] = o.band_hi;
-            sys->host_key[3] = o.variant;
+            sys->host_key[3] = o.variant + 65536.0 * o.batch_shape;
             sys->host_e = sys->d_f32;
             sys->host_g = sys->d_g32;
         }

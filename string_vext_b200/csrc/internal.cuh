@@ -181,6 +181,7 @@ struct Options {
     double band_lo, band_hi;
     int cb;
     int variant;
+    int batch_shape;   // 0 = autotune, else 1 + kernel-table index
 };
 Options resolve_options(const vext_options *opt);
 

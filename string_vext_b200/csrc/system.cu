@@ -57,6 +57,7 @@ Options resolve_options(const vext_options *opt) {
     o.band_hi = opt->band_hi;
     o.cb = opt->centers_per_region;
     o.variant = opt->variant;
+    o.batch_shape = opt->batch_shape;
     return o;
 }
 

@@ -169,3 +169,46 @@ def test_adjoint_rejects_bad_arguments():
         bad[0, 0] = np.nan
         with pytest.raises(_lib.VextError):
             system.field_adjoint_device(4, bad, e, g)
+
+
+@pytest.mark.parametrize("maker,size", [(synth.skewed_field, 5), (synth.small_field, 6)])
+def test_every_batch_shape_gives_identical_results(maker, size):
+    """Each CTA shape the autotuner may pick (pinned with batch_shape) does the
+    same per-director arithmetic in the same order: forward and forward +
+    adjoint outputs are bit-identical across shapes."""
+    case = maker()
+    _, axes = regular_pose_grid(size, 64)
+    axes = normalized_directors(axes)
+    shape = (64, size, size, size)
+    with VextSystem(case) as system:
+        ref_e, ref_g = run_device(system, size, axes, MIXED)
+        probe = VextBatch([system], size, axes,
+                          [torch.empty(shape, dtype=torch.float32, device="cuda")],
+                          gradients=[torch.empty(shape + (6,), dtype=torch.float32,
+                                                 device="cuda")])
+        n_adj = len({t["shape"] for t in probe.tuning()})
+        probe.close()
+        assert n_adj >= 5
+        for k in range(1, n_adj + 1):
+            e = torch.empty(shape, dtype=torch.float32, device="cuda")
+            g = torch.empty(shape + (6,), dtype=torch.float32, device="cuda")
+            system.field_adjoint_device(size, axes, e, g, batch_shape=k)
+            torch.cuda.synchronize()
+            np.testing.assert_array_equal(e.cpu().numpy(), ref_e)
+            np.testing.assert_array_equal(g.cpu().numpy(), ref_g)
+        fwd_ref = None
+        for k in range(1, 3):
+            out = torch.empty(shape, dtype=torch.float32, device="cuda")
+            b = VextBatch([system], size, axes, [out], batch_shape=k)
+            assert len(b.tuning()) == 1
+            b.run()
+            b.check()
+            torch.cuda.synchronize()
+            got = out.cpu().numpy()
+            if fwd_ref is None:
+                fwd_ref = got
+            np.testing.assert_array_equal(got, fwd_ref)
+            b.close()
+        with pytest.raises(_lib.VextError):
+            VextBatch([system], size, axes,
+                      [torch.empty(shape, dtype=torch.float32, device="cuda")], batch_shape=99)
