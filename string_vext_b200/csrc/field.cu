@@ -39,7 +39,6 @@ struct FieldArgs {
     const double *td;
     int n_types;
     double *e64;              // [O][S^3]
-    double *e64b;             // far sums go here instead of into e64 when non-null
     int *status;
 };
 
@@ -115,12 +114,12 @@ __global__ void __launch_bounds__(CB *G, 1) field_near_kernel(FieldArgs a) {
     }
 }
 
-// Far pairs in packed FP32x2 over every region's far entries (far_chunk,
-// pair.cuh).  A thread owns one grid center and P directors (lanes of a
-// float2 = two directors).  The far sums are added into e64 (written by the
-// near kernel) or stored into e64b.
-template <int CB, int G, int P, int MINB, bool NEWTON = true, int FLUSH = 16, bool CLO = false,
-          bool RCP3 = false>
+// The earlier far kernel (far_chunk, pair.cuh: reciprocal of q^3 with a
+// Newton step, every far entry masked), kept for comparison with
+// field_far2_kernel.  A thread owns one grid center and P directors (lanes
+// of a float2 = two directors); the far sums are added into e64 (written by
+// the near kernel).
+template <int CB, int G, int P, int MINB>
 __global__ void __launch_bounds__(CB *G, MINB) field_far_kernel(FieldArgs a) {
     static_assert(P % 2 == 0, "directors are packed in pairs");
     constexpr int NT = CB * G, PP = P / 2;
@@ -164,8 +163,7 @@ __global__ void __launch_bounds__(CB *G, MINB) field_far_kernel(FieldArgs a) {
         int start, len;
         bool near;
         plan.chunk(c, start, len, near);
-        far_chunk<P, NEWTON, FLUSH, CLO, RCP3>(st.hib + (c % kStages) * kCH, stf, len, g, ux, uy,
-                                               uz, acc);
+        far_chunk<P, true, 16>(st.hib + (c % kStages) * kCH, stf, len, g, ux, uy, uz, acc);
         stage_next(st, plan, a.hi, a.lo, c, 0);
     }
     if (cvalid) {
@@ -176,10 +174,7 @@ __global__ void __launch_bounds__(CB *G, MINB) field_far_kernel(FieldArgs a) {
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int o = obase + G * (2 * j + h);
-                if (o < a.O) {
-                    double *dst = a.e64b ? a.e64b : a.e64;   // separate buffer when run concurrently
-                    dst[(size_t)o * S3 + cg] = (a.e64b ? 0.0 : dst[(size_t)o * S3 + cg]) + acc[2 * j + h];
-                }
+                if (o < a.O) a.e64[(size_t)o * S3 + cg] += acc[2 * j + h];
             }
     }
 }
@@ -247,11 +242,7 @@ __global__ void __launch_bounds__(CB *G, MINB) field_far2_kernel(FieldArgs a) {
 #pragma unroll
         for (int p = 0; p < P; ++p) {
             const int o = obase + G * p;
-            if (o < a.O) {
-                double *dst = a.e64b ? a.e64b : a.e64;   // separate buffer when run concurrently
-                dst[(size_t)o * S3 + cg] =
-                    (a.e64b ? 0.0 : dst[(size_t)o * S3 + cg]) + acc[p] + 2.0 * shift_sum;
-            }
+            if (o < a.O) a.e64[(size_t)o * S3 + cg] += acc[p] + 2.0 * shift_sum;
         }
     }
 }
@@ -610,39 +601,18 @@ static int launch_near(const FieldArgs &a, int cb, int mode, cudaStream_t stream
     return launch_t(field_near_kernel<16, 16, 4, 2>, grid, 256, smem, a, stream);
 }
 
-// Far-kernel variants (threads = CB x G, directors per CTA = G x P):
-//   0 (default): field_far2_kernel <16, 8, 4>, 4 CTAs/SM of 128: inner entries
-//      without the cutoff mask, reciprocal of q per lane cubed, no Newton step
-//   9: field_far_kernel <16, 8, 4>: reciprocal of q^3 per lane + Newton step
-//   5: the same with one reciprocal per two lanes (1/(qx qy)) and cubing
-//   1: <16, 16, 4>, 2 CTAs/SM    2: <16, 32, 2>, 1 CTA of 512/SM
-//   3: <16, 16, 2>, 3 CTAs/SM    4: <16, 16, 4>, 3 CTAs/SM
-// cb = 32 uses <32, 8, 4>.
+// Far kernels (threads = CB x G, directors per CTA = G x P = 32):
+//   default: field_far2_kernel <16, 8, 4>, 4 CTAs/SM of 128 (<32, 8, 4> for
+//            32-center regions): inner entries without the cutoff mask,
+//            reciprocal of q per lane cubed, no Newton step
+//   9:       field_far_kernel <16, 8, 4>: reciprocal of q^3 per lane + Newton
+//            step, every entry masked (the earlier kernel, for comparison)
 static int launch_far(const FieldArgs &a, int cb, int variant, cudaStream_t stream) {
     const size_t smem = far_smem(a.n_types);
-    auto grid_for = [&](int per_cta) { return dim3(a.n_regions, (a.O + per_cta - 1) / per_cta); };
-    if (cb == 32) return launch_t(field_far_kernel<32, 8, 4, 2>, grid_for(32), 256, smem, a, stream);
-    if (variant & 32)   // without the Newton step (accuracy study)
-        return launch_t(field_far_kernel<16, 16, 4, 2, false>, grid_for(64), 256, smem, a, stream);
-    if (variant == 10)  // ... without the Newton step
-        return launch_t(field_far_kernel<16, 8, 4, 4, false, 16, false, true>, grid_for(32), 128, smem, a, stream);
-    if (variant == 8)   // with the first-order centre-residual correction
-        return launch_t(field_far_kernel<16, 8, 4, 4, true, 16, true>, grid_for(32), 128, smem, a, stream);
-    if (variant & 64)   // FP32 partial sums flushed every 8 entries
-        return launch_t(field_far_kernel<16, 8, 4, 4, true, 8>, grid_for(32), 128, smem, a, stream);
-    if (variant & 128)  // ... every 4 entries
-        return launch_t(field_far_kernel<16, 8, 4, 4, true, 4>, grid_for(32), 128, smem, a, stream);
-    switch (variant) {
-    case 2: return launch_t(field_far_kernel<16, 32, 2, 1>, grid_for(64), 512, smem, a, stream);
-    case 3: return launch_t(field_far_kernel<16, 16, 2, 3>, grid_for(32), 256, smem, a, stream);
-    case 4: return launch_t(field_far_kernel<16, 16, 4, 3>, grid_for(64), 256, smem, a, stream);
-    case 1: return launch_t(field_far_kernel<16, 16, 4, 2>, grid_for(64), 256, smem, a, stream);
-    case 5: return launch_t(field_far_kernel<16, 8, 4, 4>, grid_for(32), 128, smem, a, stream);
-    case 9:
-        return launch_t(field_far_kernel<16, 8, 4, 4, true, 16, false, true>, grid_for(32), 128,
-                        smem, a, stream);
-    default: return launch_t(field_far2_kernel<16, 8, 4, 4>, grid_for(32), 128, smem, a, stream);
-    }
+    const dim3 grid(a.n_regions, (a.O + 31) / 32);
+    if (cb == 32) return launch_t(field_far2_kernel<32, 8, 4, 2>, grid, 256, smem, a, stream);
+    if (variant == 9) return launch_t(field_far_kernel<16, 8, 4, 4>, grid, 128, smem, a, stream);
+    return launch_t(field_far2_kernel<16, 8, 4, 4>, grid, 128, smem, a, stream);
 }
 
 static FieldArgs make_args(System *sys, const RegionSet *rs, int n_axes, const double *d_axes,
@@ -669,20 +639,11 @@ static FieldArgs make_args(System *sys, const RegionSet *rs, int n_axes, const d
     a.td = sys->d_td;
     a.n_types = sys->n_types;
     a.e64 = d_e64;
-    a.e64b = nullptr;
     a.status = sys->d_status;
     return a;
 }
 
-__global__ void add_kernel(double *dst, const double *src, long long n) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x)
-        dst[i] += src[i];
-}
-
-// variant & 16: near (FP64 pipe) and far (FP32 pipe) kernels on two streams
-// so their CTAs share the SMs; far sums land in a second buffer and are added
-// afterwards.  Otherwise the far kernel runs after the near one and adds in place.
+// The near kernel writes e64, the far kernel adds its sums to it.
 int launch_field(System *sys, const RegionSet *rs, int n_axes, const double *d_axes,
                  double *d_e64, int cb, int variant, cudaStream_t stream) {
     FieldArgs a = make_args(sys, rs, n_axes, d_axes, d_e64);
@@ -701,29 +662,11 @@ int launch_field(System *sys, const RegionSet *rs, int n_axes, const double *d_a
     // near pairs are at most r_split + 2 (rho + max|offset|) apart
     double rho = 0;
     for (const RegionInfo &r : rs->h_info) rho = std::max(rho, r.rho);
-    int near_mode = rs->r_split + 2.0 * (rho + sys->max_offset) + 1e-6 < sys->cutoff ? 2 : 1;
-    if (variant & 256) near_mode = 1;   // keep the cutoff test (study)
-    variant &= ~256;
-    if (!(variant & 16)) {
-        VEXT_TRY(launch_near(a, cb, near_mode, stream));
-        VEXT_CUDA(cudaEventRecord(sys->ev[5], stream));   // near | far split of the timing
-        sys->split_timed = true;
-        return launch_far(a, cb, variant, stream);
-    }
-    variant &= ~16;
-    const size_t n = (size_t)rs->size * rs->size * rs->size * n_axes;
-    VEXT_TRY(ensure_capacity(sys->d_e64b, sys->e64b_cap, n));
-    VEXT_CUDA(cudaEventRecord(sys->fork, stream));
-    VEXT_CUDA(cudaStreamWaitEvent(sys->aux, sys->fork, 0));
+    const int near_mode = rs->r_split + 2.0 * (rho + sys->max_offset) + 1e-6 < sys->cutoff ? 2 : 1;
     VEXT_TRY(launch_near(a, cb, near_mode, stream));
-    FieldArgs b = a;
-    b.e64b = sys->d_e64b;
-    VEXT_TRY(launch_far(b, cb, variant, sys->aux));
-    VEXT_CUDA(cudaEventRecord(sys->join, sys->aux));
-    VEXT_CUDA(cudaStreamWaitEvent(stream, sys->join, 0));
-    add_kernel<<<1184, 256, 0, stream>>>(d_e64, sys->d_e64b, (long long)n);
-    VEXT_CUDA(cudaGetLastError());
-    return 0;
+    VEXT_CUDA(cudaEventRecord(sys->ev[5], stream));   // near | far split of the timing
+    sys->split_timed = true;
+    return launch_far(a, cb, variant, stream);
 }
 
 // Everything on device pointers and `stream`; region lists are built (with

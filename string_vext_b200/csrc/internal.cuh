@@ -109,10 +109,7 @@ struct System {
     PoseBatchSys h_pose_desc;
     long long *d_pose_offsets = nullptr;
     cudaStream_t stream = nullptr;   // private stream for host-pointer entries
-    cudaStream_t aux = nullptr;      // second stream: near pairs beside far pairs
-    cudaEvent_t fork = nullptr, join = nullptr;
-    double *d_e64b = nullptr;        // far-pair sums when both kernels run at once
-    size_t e64b_cap = 0;
+    cudaStream_t aux = nullptr;      // second stream: copy-back beside pair work
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     bool timed = false;              // ev[0..2] hold the last field call's kernel/epilogue
     bool list_timed = false;         // ev[3..4] hold the last list build

@@ -178,7 +178,6 @@ __device__ __forceinline__ void near_chunk(const double *ed, const double *std4,
 
 struct FarGeom {
     float cx, cy, cz;          // grid center (FP32) relative to the region origin
-    float cxl, cyl, czl;       // its FP32 rounding residual (CLO variant)
     float2 m0, m1;             // -2 o_s, broadcast
     float oo0, oo1;            // o_s^2
     float rc2f;
@@ -190,9 +189,6 @@ __device__ __forceinline__ FarGeom far_geom(double cxd, double cyd, double czd, 
     g.cx = (float)cxd;
     g.cy = (float)cyd;
     g.cz = (float)czd;
-    g.cxl = (float)(cxd - g.cx);
-    g.cyl = (float)(cyd - g.cy);
-    g.czl = (float)(czd - g.cz);
     g.m0 = make_float2(-2.f * (float)off0, -2.f * (float)off0);
     g.m1 = make_float2(-2.f * (float)off1, -2.f * (float)off1);
     g.oo0 = (float)(off0 * off0);
@@ -201,19 +197,13 @@ __device__ __forceinline__ FarGeom far_geom(double cxd, double cyd, double czd, 
     return g;
 }
 
-// Sum one staged far chunk (hi only) into acc[p] (both sites) for the
-// thread's P directors, packed two per float2 (lanes = directors p, p + 1).
-// Per entry x:  d0 = x - c, D = |d0|^2 (scalar, once; with CLO corrected by
-// -2 d0 . c_lo), t = d0 . u (packed), q_s = (D + o_s^2) - 2 o_s t.
-//   RCP3: n3 = hardware reciprocal of -q^3 per lane, refined (NEWTON) by
-//         n3' = n3 + n3 (1 + q^3 n3);
-//   else: one reciprocal per two lanes nr = 1/(-q.x q.y), n = (q.y nr, q.x nr)
-//         = -1/q, refined likewise, n3 = n^3.
-// Either way n3 = -1/q^3 and e = n3 (c12 n3 + c6) + shift = c12/q^6 -
-// c6/q^3 + shift; a 1/0 mask (q < rc^2) multiplies e into FP32 partial sums
-// flushed into FP64 every FLUSH entries.  Far entries are >= r_split from
-// every site, so no pair reaches the contact floor (no max()).
-template <int P, bool NEWTON, int FLUSH, bool CLO, bool RCP3>
+// The earlier forward far chunk, kept for comparison with far_chunk_fwd:
+// per lane n3 = hardware reciprocal of -q^3, refined (NEWTON) by n3' = n3 +
+// n3 (1 + q^3 n3); e = n3 (c12 n3 + c6) + shift = c12/q^6 - c6/q^3 + shift;
+// a 1/0 mask (q < rc^2) multiplies e into FP32 partial sums flushed into FP64
+// every FLUSH entries.  Far entries are >= r_split from every site, so no
+// pair reaches the contact floor (no max()).
+template <int P, bool NEWTON, int FLUSH>
 __device__ __forceinline__ void far_chunk(const float4 *hb, const float4 *stf, int len,
                                           const FarGeom &g, const float2 (&ux)[P / 2],
                                           const float2 (&uy)[P / 2], const float2 (&uz)[P / 2],
@@ -231,8 +221,7 @@ __device__ __forceinline__ void far_chunk(const float4 *hb, const float4 *stf, i
             const float4 h = hb[e];
             const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, floor2)
             const float dx = h.x - g.cx, dy = h.y - g.cy, dz = h.z - g.cz;
-            float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            if (CLO) dd = fmaf(-2.f, fmaf(dx, g.cxl, fmaf(dy, g.cyl, dz * g.czl)), dd);
+            const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             const float2 k0 = make_float2(dd + g.oo0, dd + g.oo0),
                          k1 = make_float2(dd + g.oo1, dd + g.oo1);
             const float2 dx2 = make_float2(dx, dx), dy2 = make_float2(dy, dy),
@@ -246,21 +235,12 @@ __device__ __forceinline__ void far_chunk(const float4 *hb, const float4 *stf, i
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
                     const float2 d2 = __ffma2_rn(q ? g.m1 : g.m0, t, q ? k1 : k0);
-                    float2 n3;
-                    if (RCP3) {
-                        const float2 d6 = __fmul2_rn(__fmul2_rn(d2, d2), d2);
-                        float r0, r1;
-                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(-d6.x));
-                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r1) : "f"(-d6.y));
-                        n3 = make_float2(r0, r1);
-                        if (NEWTON) n3 = __ffma2_rn(n3, __ffma2_rn(d6, n3, one2), n3);
-                    } else {
-                        float nr;
-                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(nr) : "f"(-d2.x * d2.y));
-                        float2 n = make_float2(d2.y * nr, d2.x * nr);
-                        if (NEWTON) n = __ffma2_rn(n, __ffma2_rn(d2, n, one2), n);
-                        n3 = __fmul2_rn(__fmul2_rn(n, n), n);
-                    }
+                    const float2 d6 = __fmul2_rn(__fmul2_rn(d2, d2), d2);
+                    float r0, r1;
+                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(-d6.x));
+                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r1) : "f"(-d6.y));
+                    float2 n3 = make_float2(r0, r1);
+                    if (NEWTON) n3 = __ffma2_rn(n3, __ffma2_rn(d6, n3, one2), n3);
                     const float2 en = __ffma2_rn(n3, __ffma2_rn(c12, n3, c6), sh);
                     const float2 m = make_float2(set_lt(d2.x, g.rc2f), set_lt(d2.y, g.rc2f));
                     fa[j] = __ffma2_rn(en, m, fa[j]);

@@ -464,9 +464,6 @@ System::~System() {
     cudaFree(d_pose_offsets);
     for (auto &e : ev)
         if (e) cudaEventDestroy(e);
-    if (fork) cudaEventDestroy(fork);
-    if (join) cudaEventDestroy(join);
-    cudaFree(d_e64b);
     if (aux) cudaStreamDestroy(aux);
     if (stream) cudaStreamDestroy(stream);
 }
@@ -581,8 +578,6 @@ extern "C" int vext_system_create(const vext_system_desc *d, vext_system *out) {
     };
     chk(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
     chk(cudaStreamCreateWithFlags(&s.aux, cudaStreamNonBlocking));
-    chk(cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming));
-    chk(cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming));
     for (auto &e : s.ev) chk(cudaEventCreate(&e));
     chk(cudaMalloc(&s.d_frac, sizeof(double) * frac.size()));
     chk(cudaMalloc(&s.d_type, sizeof(int) * type.size()));
