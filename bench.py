@@ -408,7 +408,7 @@ def secondary_measurements(args, system, case, size, axes, poses, pairs, far_pai
                 "float32 epilogue",
         "breakdown_ms": {"list_build": list_ms, "near_pairs_fp64": near_ms,
                          "far_pairs_fp32x2": far_ms, "refine_epilogue": epi_ms},
-        "roofline_far_kernel": {"kernel": "field_far2_kernel<16,8,4,4>", "bound": "fp32",
+        "roofline_far_kernel": {"kernel": "field_far2_kernel<16,8,4,6>", "bound": "fp32",
                                 "achieved": achieved_far / 1e12, "peak": peak / 1e12,
                                 "unit": "TFLOP/s", "frac": achieved_far / peak,
                                 "algorithmic": f"{far_pairs} far in-cutoff pairs x {FLOP_FWD} FLOP",

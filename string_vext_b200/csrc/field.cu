@@ -602,7 +602,7 @@ static int launch_near(const FieldArgs &a, int cb, int mode, cudaStream_t stream
 }
 
 // Far kernels (threads = CB x G, directors per CTA = G x P = 32):
-//   default: field_far2_kernel <16, 8, 4>, 4 CTAs/SM of 128 (<32, 8, 4> for
+//   default: field_far2_kernel <16, 8, 4>, 6 CTAs/SM of 128 (<32, 8, 4> for
 //            32-center regions): inner entries without the cutoff mask,
 //            reciprocal of q per lane cubed, no Newton step
 //   9:       field_far_kernel <16, 8, 4>: reciprocal of q^3 per lane + Newton
@@ -612,7 +612,7 @@ static int launch_far(const FieldArgs &a, int cb, int variant, cudaStream_t stre
     const dim3 grid(a.n_regions, (a.O + 31) / 32);
     if (cb == 32) return launch_t(field_far2_kernel<32, 8, 4, 2>, grid, 256, smem, a, stream);
     if (variant == 9) return launch_t(field_far_kernel<16, 8, 4, 4>, grid, 128, smem, a, stream);
-    return launch_t(field_far2_kernel<16, 8, 4, 4>, grid, 128, smem, a, stream);
+    return launch_t(field_far2_kernel<16, 8, 4, 6>, grid, 128, smem, a, stream);
 }
 
 static FieldArgs make_args(System *sys, const RegionSet *rs, int n_axes, const double *d_axes,
