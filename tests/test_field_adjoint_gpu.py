@@ -212,3 +212,34 @@ def test_every_batch_shape_gives_identical_results(maker, size):
         with pytest.raises(_lib.VextError):
             VextBatch([system], size, axes,
                       [torch.empty(shape, dtype=torch.float32, device="cuda")], batch_shape=99)
+
+
+@pytest.mark.parametrize("size,n_axes", [(1, 7), (3, 33), (2, 40), (5, 1)])
+def test_ragged_grids_and_director_counts(size, n_axes):
+    """Director counts that are not multiples of the 32-director block (one
+    more than a block: the host entry's split), a one-point grid, a single
+    director: device and host entries agree bit for bit and match the oracle."""
+    case = synth.small_field()
+    rng = np.random.default_rng(size * 100 + n_axes)
+    axes = normalized_directors(rng.normal(size=(n_axes, 3)))
+    frac = (np.arange(size) + .5) / size
+    grid = np.stack(np.meshgrid(frac, frac, frac, indexing="ij"), -1).reshape(-1, 3)
+    cart = grid @ np.asarray(case["cell"], dtype=float)
+    centers = np.ascontiguousarray(
+        np.broadcast_to(cart[None], (n_axes,) + cart.shape).reshape(-1, 3))
+    dirs = np.ascontiguousarray(
+        np.broadcast_to(axes[:, None, :], (n_axes, len(cart), 3)).reshape(-1, 3))
+    e_ref, gc, gu = oracle.pose_energy_grad(case, centers, dirs)
+    gu = gu - (gu * dirs).sum(1)[:, None] * dirs
+    g_ref = np.concatenate([gc, gu], 1)
+    with VextSystem(case) as system:
+        de, dg, de64 = run_device(system, size, axes, MIXED, energy64=True)
+        he, hg = system.field_adjoint(size, axes)
+    np.testing.assert_array_equal(he, de)
+    np.testing.assert_array_equal(hg, dg)
+    e = de64.reshape(-1)
+    neg = e_ref <= 0
+    if neg.any():
+        assert np.abs(e - e_ref)[neg].max() < 1e-4
+    assert (np.abs(e - e_ref) / np.maximum(np.abs(e_ref), 1))[~neg].max() < 1e-6
+    assert grad_rel(dg.reshape(-1, 6).astype(np.float64), g_ref).max() < 1e-5
