@@ -46,7 +46,7 @@ FLOP_FWD_ADJ = 28      # forward + adjoint
 METRIC = "Vext pose evals/s at <=1e-4 K vs FP64, fwd+adjoint evals/s; % FP32 peak"
 # dram__bytes_read.sum + dram__bytes_write.sum of one field_far2_kernel launch on
 # full_field, from an ncu capture (--set full) of `bench.py --profile field`.
-FAR_DRAM_BYTES_FULL_FIELD = 743_810_048 + 100_710_144
+FAR_DRAM_BYTES_FULL_FIELD = 744_213_504 + 100_719_360
 # the same for one forward + adjoint batch_field_kernel launch on full_field,
 # from an ncu capture (--set full) of `bench.py --profile adjoint`.
 ADJ_DRAM_BYTES_FULL_FIELD = 423_897_344 + 352_798_720
