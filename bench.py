@@ -480,7 +480,21 @@ def secondary_measurements(args, system, case, size, axes, poses, pairs, far_pai
     out["pose_fwd_adjoint"] = {"value": n_pose / (pose_ms * 1e-3), "unit": "poses/s",
                                "poses": n_pose, "workload": "random poses (center, quaternion), "
                                "same framework", "flop_per_pair": FLOP_FWD_ADJ}
-    del cart, q, e, gc, gq
+    # error of the pose path against its FP64 mode on the same poses
+    e64p, gc64, gq64 = torch.empty_like(e), torch.empty_like(gc), torch.empty_like(gq)
+    system.pose_energy_grad_device(cart, q, e64p, gc64, gq64, mode=_lib.VEXT_MODE_FP64,
+                                   stream=stream)
+    torch.cuda.synchronize()
+    perr = error_stats(e.cpu().numpy(), e64p.cpu().numpy())
+    for name, mixed, exact in (("center", gc, gc64), ("quaternion", gq, gq64)):
+        gx, gm = exact.cpu().numpy(), mixed.cpu().numpy()
+        grel = np.linalg.norm(gm - gx, axis=-1) / np.maximum(np.linalg.norm(gx, axis=-1), 1.0)
+        perr[f"gradient_{name}_max_rel"] = float(grel.max())
+        perr[f"gradient_{name}_median_rel"] = float(np.median(grel))
+    perr["reference"] = ("the pose path's FP64 mode (every pair in FP64, correctly rounded "
+                         "reciprocal) on the same poses")
+    out["pose_fwd_adjoint"]["error_vs_fp64"] = perr
+    del cart, q, e, gc, gq, e64p, gc64, gq64
     out["precision_study"] = precision_study(device)
     out["string_update"] = bench_string_update()
     if not args.no_batch:

@@ -16,7 +16,7 @@
 #include <algorithm>
 #include <cmath>
 
-#include "stage.cuh"
+#include "pair.cuh"
 
 namespace vext {
 
@@ -174,7 +174,73 @@ __device__ __forceinline__ void write_pose(const PoseArgs &a, int p, double e, c
     }
 }
 
-template <int NT>
+// Far entries [e_begin, e_end) of one staged chunk for one pose: the packed
+// FP32x2 loop of the field kernels with the lanes holding the pose's two
+// sites.  Per lane d = x - r_s, n1 = hardware reciprocal of d2, n3 = n1^3,
+// e = n3 (c12 n3 - c6), fp = (n1 n3)(c6 - 2 c12 n3) = (dE/dd2) / 3 and
+// G_s += fp d, so that dE/dr_s = -6 G_s.  Far entries lie beyond r_split of
+// every site of every pose of the bin, so the contact floor never applies.
+// MASK = false for inner entries (inside the cutoff of every such site): no
+// cutoff mask, and the shift is summed once per entry into shift_sum (added
+// to both sites).  Energy partials are flushed into FP64 every 16 entries,
+// the gradient partials once per call.
+template <bool MASK>
+__device__ __forceinline__ void pose_far(const float4 *hb, const float4 *stf, int e_begin,
+                                         int e_end, float2 nsx, float2 nsy, float2 nsz,
+                                         float rc2f, double (&E)[2], double (&F)[2][3],
+                                         double &shift_sum) {
+    float2 gx = make_float2(0.f, 0.f), gy = gx, gz = gx;
+#pragma unroll 1
+    for (int e0 = e_begin; e0 < e_end; e0 += 16) {
+        float2 fe = make_float2(0.f, 0.f);
+        float fs = 0.f;
+        const int e1 = min(e0 + 16, e_end);
+#pragma unroll 2
+        for (int e = e0; e < e1; ++e) {
+            const float4 h = hb[e];
+            const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, floor2)
+            const float2 dx = __fadd2_rn(make_float2(h.x, h.x), nsx),
+                         dy = __fadd2_rn(make_float2(h.y, h.y), nsy),
+                         dz = __fadd2_rn(make_float2(h.z, h.z), nsz);
+            const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+            float r0, r1;
+            asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(d2.x));
+            asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r1) : "f"(d2.y));
+            const float2 n1 = make_float2(r0, r1);
+            float2 n3 = __fmul2_rn(__fmul2_rn(n1, n1), n1);
+            if (MASK) {
+                const float2 m = make_float2(set_lt(d2.x, rc2f), set_lt(d2.y, rc2f));
+                n3 = __fmul2_rn(n3, m);
+                fe = __ffma2_rn(m, make_float2(tp.z, tp.z), fe);
+            } else {
+                fs += tp.z;
+            }
+            fe = __ffma2_rn(n3, __ffma2_rn(make_float2(tp.x, tp.x), n3, make_float2(-tp.y, -tp.y)),
+                            fe);
+            const float2 fp =
+                __fmul2_rn(__fmul2_rn(n1, n3),
+                           __ffma2_rn(make_float2(-2.f * tp.x, -2.f * tp.x), n3,
+                                      make_float2(tp.y, tp.y)));
+            gx = __ffma2_rn(fp, dx, gx);
+            gy = __ffma2_rn(fp, dy, gy);
+            gz = __ffma2_rn(fp, dz, gz);
+        }
+        E[0] += (double)fe.x;
+        E[1] += (double)fe.y;
+        if (!MASK) shift_sum += (double)fs;
+    }
+    F[0][0] -= 6.0 * (double)gx.x;
+    F[1][0] -= 6.0 * (double)gx.y;
+    F[0][1] -= 6.0 * (double)gy.x;
+    F[1][1] -= 6.0 * (double)gy.y;
+    F[0][2] -= 6.0 * (double)gz.x;
+    F[1][2] -= 6.0 * (double)gz.y;
+}
+
+// MIXED: near pairs take the FP64 reciprocal as a hardware seed + one Newton
+// step (relative error <= 2^-46) and far pairs the packed FP32 loop; otherwise
+// (the FP64 mode: every entry is near) the correctly rounded reciprocal.
+template <int NT, bool MIXED>
 __global__ void __launch_bounds__(NT) pose_kernel(PoseArgs a) {
     const int item = blockIdx.x;
     if (item >= a.items[0]) return;   // uniform over the CTA
@@ -213,17 +279,18 @@ __global__ void __launch_bounds__(NT) pose_kernel(PoseArgs a) {
                  cx, cy, cz);
     const double ux = a.u[3 * p], uy = a.u[3 * p + 1], uz = a.u[3 * p + 2];
     double sd[2][3];
-    float sf[2][3];
-    double E[2] = {0, 0}, F[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    double E[2] = {0, 0}, F[2][3] = {{0, 0, 0}, {0, 0, 0}}, shift_sum = 0.0;
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
         const double off = s ? a.off1 : a.off0;
         sd[s][0] = cx + off * ux;
         sd[s][1] = cy + off * uy;
         sd[s][2] = cz + off * uz;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) sf[s][k] = (float)sd[s][k];
     }
+    // the sites negated, one per lane, for the far loop's d = x - r_s
+    const float2 nsx = make_float2(-(float)sd[0][0], -(float)sd[1][0]),
+                 nsy = make_float2(-(float)sd[0][1], -(float)sd[1][1]),
+                 nsz = make_float2(-(float)sd[0][2], -(float)sd[1][2]);
 
     for (int c = 0; c < plan.n_chunks; ++c) {
         const int s = c % kStages;
@@ -260,7 +327,7 @@ __global__ void __launch_bounds__(NT) pose_kernel(PoseArgs a) {
                     const double dx = sd[q][0] - xy.x, dy = sd[q][1] - xy.y, dz = sd[q][2] - zt.x;
                     const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
                     const double s2 = fmax(d2, sh.y);
-                    const double i2 = __drcp_rn(s2);
+                    const double i2 = MIXED ? rcp64_nr<1>(s2) : __drcp_rn(s2);
                     const double i6 = i2 * i2 * i2;
                     const double en = fma(i6, fma(cc.x, i6, -cc.y), sh.x);
                     const bool in = d2 < a.rc2;
@@ -271,47 +338,19 @@ __global__ void __launch_bounds__(NT) pose_kernel(PoseArgs a) {
                     F[q][2] = fma(w, dz, F[q][2]);
                 }
             }
-        } else {
+        } else if (MIXED) {
+            // inner entries first, then the shell (the chunk may straddle them)
             const float4 *hb = st.hib + s * kCH;
-#pragma unroll 1
-            for (int e0 = 0; e0 < len; e0 += 16) {
-                float fe[2] = {0.f, 0.f}, ff[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
-                const int e1 = min(e0 + 16, len);
-#pragma unroll 2
-                for (int e = e0; e < e1; ++e) {
-                    const float4 h = hb[e];
-                    const float4 tp = stf[__float_as_int(h.w)];
-                    const float a12 = -12.0f * tp.x, a6 = 6.0f * tp.y;
-#pragma unroll
-                    for (int q = 0; q < 2; ++q) {
-                        const float dx = sf[q][0] - h.x, dy = sf[q][1] - h.y, dz = sf[q][2] - h.z;
-                        const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                        const float s2 = fmaxf(d2, tp.w);
-                        const float i2 = rcp_nr(s2);
-                        const float i6 = i2 * i2 * i2;
-                        const float en = fmaf(i6, fmaf(tp.x, i6, -tp.y), tp.z);
-                        const bool in = d2 < a.rc2f;
-                        const float w = (in && d2 > tp.w) ? i2 * i6 * fmaf(a12, i6, a6) : 0.f;
-                        fe[q] += in ? en : 0.f;
-                        ff[q][0] = fmaf(w, dx, ff[q][0]);
-                        ff[q][1] = fmaf(w, dy, ff[q][1]);
-                        ff[q][2] = fmaf(w, dz, ff[q][2]);
-                    }
-                }
-#pragma unroll
-                for (int q = 0; q < 2; ++q) {
-                    E[q] += (double)fe[q];
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) F[q][k] += (double)ff[q][k];
-                }
-            }
+            const int split = min(max(r.n_near + r.n_inner - start, 0), len);
+            pose_far<false>(hb, stf, 0, split, nsx, nsy, nsz, a.rc2f, E, F, shift_sum);
+            pose_far<true>(hb, stf, split, len, nsx, nsy, nsz, a.rc2f, E, F, shift_sum);
         }
         __syncthreads();
         if (tid == 0 && c + kStages < plan.n_chunks)
             st.issue(plan, a.hi, a.lo, c + kStages, c + kStages);
     }
     if (valid) {
-        const double e = E[0] + E[1];
+        const double e = E[0] + E[1] + 2.0 * shift_sum;
         write_pose(a, p, e, F[0], F[1]);
         if (a.refine && e > a.band_lo && e < a.band_hi) {
             const int k = atomicAdd(&a.refine[0], 1);
@@ -482,9 +521,10 @@ int pose_enqueue(System *sys, int n, const double *centers, const double *quats,
     pose_scatter_kernel<<<pb, 256, 0, st>>>(a);
     VEXT_CUDA(cudaGetLastError());
     const size_t smem = kStageBytes + (size_t)kCH * 4 * sizeof(double) + (size_t)a.n_types * 48;
-    VEXT_CUDA(cudaFuncSetAttribute(pose_kernel<kPoseThreads>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    pose_kernel<kPoseThreads><<<max_items, kPoseThreads, smem, st>>>(a);
+    auto kernel = o.mode == VEXT_MODE_MIXED ? pose_kernel<kPoseThreads, true>
+                                            : pose_kernel<kPoseThreads, false>;
+    VEXT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kernel<<<max_items, kPoseThreads, smem, st>>>(a);
     VEXT_CUDA(cudaGetLastError());
     if (refine) {
         pose_refine_kernel<<<std::min(1184, (n + 7) / 8), 256, 0, st>>>(a);
