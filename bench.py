@@ -347,7 +347,9 @@ def run_ours(args, rank, world, local_rank):
                     "region lists resident (built once per framework, reported as setup)",
             "e2e": {"value": e2e_value, "unit": "poses/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
-                    "path": "vext_field_adjoint (host pinned float32 energy + gradient)"},
+                    "path": "vext_field_adjoint into page-locked host float32 energy + "
+                            "gradient (the kernels write them over PCIe during the pair "
+                            "work)"},
             "gpu_launches": args.steps * 2,
             "setup_s": setup_s,
             "roofline": {"bound": "fp32",

@@ -19,6 +19,7 @@
 // keeps pointers to its systems' region lists: the systems must outlive it
 // and not be invalidated while it exists.
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <memory>
 #include <numeric>
@@ -470,6 +471,7 @@ struct vext_batch_s {
     int size = 0, n_axes = 0;
     Options opt;
     BatchSys *d_sys = nullptr;
+    std::vector<std::pair<float *, float *>> targets;   // current (out, grad) of each system
     int4 *d_items = nullptr, *d_sample = nullptr;
     int n_items = 0, n_sample = 0;
     int *d_counter = nullptr, *d_refine = nullptr;
@@ -626,6 +628,7 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
     std::vector<int4> sample;
     for (size_t i = 0; i < hitems.size(); i += 16) sample.push_back(hitems[i]);
     b->n_sample = (int)sample.size();
+    for (const BatchSys &y : hs) b->targets.push_back({y.out, y.grad});
     VEXT_CUDA(cudaMalloc(&b->d_sys, sizeof(BatchSys) * n_systems));
     VEXT_CUDA(cudaMemcpy(b->d_sys, hs.data(), sizeof(BatchSys) * n_systems, cudaMemcpyHostToDevice));
     VEXT_CUDA(cudaMalloc(&b->d_items, sizeof(int4) * hitems.size()));
@@ -727,6 +730,22 @@ namespace vext {
 // Replay on exactly `stream` (0 = the legacy default stream).
 int batch_replay(vext_batch b, cudaStream_t stream) {
     VEXT_CUDA(cudaGraphLaunch(b->exec, stream));
+    return 0;
+}
+
+// Point system k's float32 energy / gradient outputs at `out` / `grad` for the
+// replays that follow on `stream`: a stream-ordered update of the device copy
+// of its BatchSys, which the captured kernels read at run time (no rebuild).
+int batch_retarget(vext_batch b, int k, float *out, float *grad, cudaStream_t stream) {
+    if (k < 0 || k >= (int)b->systems.size()) return fail(VEXT_ERR_ARGUMENT, "bad system index");
+    if (!out || (b->adj && !grad)) return fail(VEXT_ERR_ARGUMENT, "null output");
+    static_assert(offsetof(BatchSys, grad) == offsetof(BatchSys, out) + sizeof(float *),
+                  "out and grad must be adjacent");
+    float *ptrs[2] = {out, b->adj ? grad : nullptr};
+    if (b->targets[k].first == ptrs[0] && b->targets[k].second == ptrs[1]) return 0;
+    VEXT_CUDA(cudaMemcpyAsync(reinterpret_cast<char *>(b->d_sys + k) + offsetof(BatchSys, out),
+                              ptrs, sizeof ptrs, cudaMemcpyHostToDevice, stream));
+    b->targets[k] = {ptrs[0], ptrs[1]};
     return 0;
 }
 

@@ -17,6 +17,8 @@
 #include <algorithm>
 #include <cmath>
 
+#include <cuda.h>
+
 #include "pair.cuh"
 
 namespace vext {
@@ -830,10 +832,10 @@ static int field_adjoint_device(vext_system h, int size, int n_axes, const doubl
                           sys->adj_key[0] == o.r_split && sys->adj_key[1] == o.band_lo &&
                           sys->adj_key[2] == o.band_hi &&
                           sys->adj_key[3] == o.variant + 65536.0 * o.batch_shape &&
-                          sys->adj_energy == energy &&
-                          sys->adj_grad == gradient && sys->adj_energy64 == energy_f64;
+                          sys->adj_energy64 == energy_f64;
         if (!same) {
-            sys->drop_adjoint_batch();
+            if (sys->adj_batch) vext_batch_destroy(sys->adj_batch);   // (host parts stay)
+            sys->adj_batch = nullptr;
             vext_batch b = nullptr;
             VEXT_TRY(batch_build(1, &h, size, n_axes, axes, opt, &energy, &gradient,
                                  energy_f64 ? &energy_f64 : nullptr, false, &b));
@@ -844,10 +846,11 @@ static int field_adjoint_device(vext_system h, int size, int n_axes, const doubl
             sys->adj_key[1] = o.band_lo;
             sys->adj_key[2] = o.band_hi;
             sys->adj_key[3] = o.variant + 65536.0 * o.batch_shape;
-            sys->adj_energy = energy;
-            sys->adj_grad = gradient;
             sys->adj_energy64 = energy_f64;
         }
+        // other float32 outputs than the last call's: a stream-ordered update
+        // of the batch's output pointers, no rebuild
+        VEXT_TRY(batch_retarget(sys->adj_batch, 0, energy, gradient, stream));
         return batch_replay(sys->adj_batch, stream);
     }
     if (o.mode != VEXT_MODE_FP64 && o.mode != VEXT_MODE_FP64_PLAIN)
@@ -879,6 +882,45 @@ extern "C" int vext_field_adjoint_device(vext_system h, int size, int n_axes,
                                 gradient_f64, (cudaStream_t)stream);
 }
 
+// Device address of host memory the kernels may write directly: [p, p +
+// bytes) must lie inside one page-locked, device-mapped allocation (checked
+// by the driver's allocation range of p and by the mapping of the last byte);
+// otherwise null, and the caller copies through device memory instead.
+static void *mapped_host_range(void *p, size_t bytes) {
+    using RangeFn = CUresult (*)(void *, CUpointer_attribute, CUdeviceptr);
+    static RangeFn range_fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuPointerGetAttribute", &f, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (RangeFn) nullptr;
+        }
+        return reinterpret_cast<RangeFn>(f);
+    }();
+    if (!range_fn || !p || bytes == 0) return nullptr;
+    cudaPointerAttributes first, last;
+    if (cudaPointerGetAttributes(&first, p) != cudaSuccess ||
+        cudaPointerGetAttributes(&last, static_cast<char *>(p) + bytes - 1) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (first.type != cudaMemoryTypeHost || last.type != cudaMemoryTypeHost ||
+        !first.devicePointer ||
+        static_cast<char *>(last.devicePointer) !=
+            static_cast<char *>(first.devicePointer) + (bytes - 1))
+        return nullptr;
+    const CUdeviceptr d = reinterpret_cast<CUdeviceptr>(first.devicePointer);
+    CUdeviceptr start = 0;
+    size_t range = 0;
+    if (range_fn(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, d) != CUDA_SUCCESS ||
+        range_fn(&range, CU_POINTER_ATTRIBUTE_RANGE_SIZE, d) != CUDA_SUCCESS)
+        return nullptr;
+    if (d < start || d - start > range || bytes > range - (d - start)) return nullptr;
+    return first.devicePointer;
+}
+
 extern "C" int vext_field_adjoint(vext_system h, int size, int n_axes, const double *axes,
                                   const vext_options *opt, float *energy, float *gradient) {
     if (!h) return fail(VEXT_ERR_ARGUMENT, "null system");
@@ -892,9 +934,23 @@ extern "C" int vext_field_adjoint(vext_system h, int size, int n_axes, const dou
     VEXT_TRY(ensure_capacity(sys->d_f32, sys->f32_cap, n));
     VEXT_TRY(ensure_capacity(sys->d_g32, sys->g32_cap, 6 * n));
     cudaStream_t st = sys->stream;
-    if (o.mode == VEXT_MODE_MIXED && n_axes > 32) {
-        // one batch per 32-director block; block k's copy (on aux) overlaps
-        // block k + 1's pair work (on st)
+    if (o.mode == VEXT_MODE_MIXED) {
+        // page-locked host outputs: one batch over all directors writes the
+        // float32 results straight into them (the transfer runs beside the
+        // pair work)
+        float *de = static_cast<float *>(mapped_host_range(energy, sizeof(float) * n));
+        float *dg = de ? static_cast<float *>(mapped_host_range(gradient, sizeof(float) * 6 * n))
+                       : nullptr;
+        if (de && dg) {
+            VEXT_TRY(field_adjoint_device(h, size, n_axes, axes, o, opt, de, dg, nullptr, nullptr,
+                                          st));
+            VEXT_CUDA(cudaStreamSynchronize(st));
+            return vext_batch_status(sys->adj_batch);
+        }
+    }
+    if (o.mode == VEXT_MODE_MIXED) {
+        // pageable host outputs: one batch per 32-director block; block k's
+        // copy (on aux) overlaps block k + 1's pair work (on st)
         for (int k = 0; k < 3 * n_axes; ++k)
             if (!std::isfinite(axes[k])) return fail(VEXT_ERR_ARGUMENT, "non-finite director");
         const size_t S3 = (size_t)size * size * size;
@@ -951,8 +1007,7 @@ extern "C" int vext_field_adjoint(vext_system h, int size, int n_axes, const dou
     VEXT_CUDA(cudaMemcpyAsync(gradient, sys->d_g32, sizeof(float) * 6 * n,
                               cudaMemcpyDeviceToHost, st));
     VEXT_CUDA(cudaStreamSynchronize(st));
-    if (sys->adj_batch && o.mode == VEXT_MODE_MIXED) return vext_batch_status(sys->adj_batch);
-    return check_status(sys, st);
+    return check_status(sys, st);   // the FP64 modes (the mixed mode returned above)
 }
 
 extern "C" int vext_count_pairs(vext_system h, int size, int n_axes, const double *axes,

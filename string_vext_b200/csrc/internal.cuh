@@ -114,13 +114,14 @@ struct System {
     bool timed = false;              // ev[0..2] hold the last field call's kernel/epilogue
     bool list_timed = false;         // ev[3..4] hold the last list build
     bool split_timed = false;        // ev[5] separates the near and far kernels
-    // cached one-system forward + adjoint batch (vext_field_adjoint_device),
-    // keyed by grid size, directors, options and output pointers
+    // cached one-system forward + adjoint batch (vext_field_adjoint_device and
+    // vext_field_adjoint into page-locked buffers), keyed by grid size,
+    // directors, options and the FP64 energy output; its float32 outputs are
+    // retargeted per call
     vext_batch adj_batch = nullptr;
     int adj_size = 0;
     std::vector<double> adj_axes;
     double adj_key[4] = {0, 0, 0, 0};   // r_split, band_lo, band_hi, variant
-    float *adj_energy = nullptr, *adj_grad = nullptr;
     double *adj_energy64 = nullptr;
     float *d_g32 = nullptr;          // host-output staging of the float32 gradient
     size_t g32_cap = 0;
@@ -145,6 +146,7 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
                 float *const *gradients, double *const *outputs_f64, bool lock_systems,
                 vext_batch *out);
 int batch_replay(vext_batch b, cudaStream_t stream);
+int batch_retarget(vext_batch b, int k, float *out, float *grad, cudaStream_t stream);
 
 // Region sets (system.cu)
 int get_field_regions(System *sys, int size, int cb, double r_split, RegionSet **out,

@@ -243,3 +243,45 @@ def test_ragged_grids_and_director_counts(size, n_axes):
         assert np.abs(e - e_ref)[neg].max() < 1e-4
     assert (np.abs(e - e_ref) / np.maximum(np.abs(e_ref), 1))[~neg].max() < 1e-6
     assert grad_rel(dg.reshape(-1, 6).astype(np.float64), g_ref).max() < 1e-5
+
+
+def test_host_entry_into_page_locked_buffers():
+    """vext_field_adjoint with page-locked host outputs (the kernels write the
+    float32 results straight into them) gives the same bits as with pageable
+    outputs (staged copies) and as the device entry, including slices inside
+    a larger page-locked allocation, whose neighbouring words stay untouched,
+    and when calls switch between the two kinds of buffer."""
+    import ctypes
+    case = synth.small_field()
+    size, n_axes = 6, 64
+    _, axes = regular_pose_grid(size, n_axes)
+    axes = normalized_directors(axes)
+    shape = (n_axes, size, size, size)
+    n = int(np.prod(shape))
+    lib = _lib.load()
+    opt = _lib.options()
+
+    def host_call(system, e, g):
+        _lib.check(lib.vext_field_adjoint(system.handle, size, n_axes, _lib.ptr(axes),
+                                          ctypes.byref(opt), _lib.ptr(e), _lib.ptr(g)))
+
+    with VextSystem(case) as system:
+        ref_e, ref_g = run_device(system, size, axes, MIXED)
+        for _ in range(2):
+            pe = torch.full(shape, -7.0, dtype=torch.float32, pin_memory=True)
+            pg = torch.full(shape + (6,), -7.0, dtype=torch.float32, pin_memory=True)
+            host_call(system, pe, pg)
+            np.testing.assert_array_equal(pe.numpy(), ref_e)
+            np.testing.assert_array_equal(pg.numpy(), ref_g)
+            e, g = system.field_adjoint(size, axes)      # pageable numpy outputs
+            np.testing.assert_array_equal(e, ref_e)
+            np.testing.assert_array_equal(g, ref_g)
+        pad = 16
+        be = torch.full((n + 2 * pad,), -7.0, dtype=torch.float32, pin_memory=True)
+        bg = torch.full((6 * n + 2 * pad,), -7.0, dtype=torch.float32, pin_memory=True)
+        se, sg = be[pad:pad + n], bg[pad:pad + 6 * n]
+        host_call(system, se, sg)
+        np.testing.assert_array_equal(se.numpy().reshape(shape), ref_e)
+        np.testing.assert_array_equal(sg.numpy().reshape(shape + (6,)), ref_g)
+        for big in (be, bg):
+            assert (big[:pad] == -7.0).all() and (big[-pad:] == -7.0).all()
