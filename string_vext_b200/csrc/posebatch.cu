@@ -5,8 +5,9 @@
 // One warp per pose.  The pose's center is wrapped into its system's cell and
 // binned (the bin lists of system.cu, built at creation); the 32 lanes stride
 // over the bin's list: near entries in FP64 from hi + lo with the contact
-// floor, far entries in FP32 (reciprocal of d^2 per pair, cubed) with
-// per-lane FP32 partials flushed into FP64 every 16 entries.  The seven sums
+// floor, far entries in packed FP32x2 (the two sites in the two lanes;
+// reciprocal of d^2 per pair, cubed) with per-lane FP32 partials flushed into
+// FP64 every 16 entries.  The seven sums
 // (E, dE/dsite for both sites) are reduced over the warp; a pose whose energy
 // falls in the refinement band is recomputed entirely in FP64 by the same
 // warp.  Outputs as vext_pose_energy_grad: E, dE/dcenter, tangent dE/dq,
@@ -17,7 +18,7 @@
 #include <memory>
 #include <vector>
 
-#include "internal.cuh"
+#include "pair.cuh"
 
 namespace vext {
 
@@ -32,9 +33,69 @@ struct PoseBatchArgs {
     int *status;
 };
 
+// This lane's far entries begin + lane + 32 i < end of one pose, the two
+// sites in the two lanes of the packed FP32x2 instructions (pose.cu's far loop):
+// d = x - r_s, n1 = hardware reciprocal of d2, n3 = n1^3, e = n3 (c12 n3 - c6),
+// fp = (n1 n3)(c6 - 2 c12 n3), dE/dsite += -6 fp d.  MASK = false for inner
+// entries (within the cutoff of every pose of the bin: no mask, the shift
+// summed once per entry into shift_sum).  FP32 partials are flushed into the
+// FP64 sums every 16 entries.
+template <bool MASK>
+__device__ __forceinline__ void far_lane_sums(const PoseBatchSys &y, long long base, int begin,
+                                              int end, int lane, float2 nsx, float2 nsy,
+                                              float2 nsz, double (&v)[7], double &shift_sum) {
+    const int mine = end - begin > lane ? (end - begin - lane + 31) / 32 : 0;
+#pragma unroll 1
+    for (int i0 = 0; i0 < mine; i0 += 16) {
+        float2 fe = make_float2(0.f, 0.f), gx = fe, gy = fe, gz = fe;
+        float fs = 0.f;
+        const int i1 = min(i0 + 16, mine);
+        for (int i = i0; i < i1; ++i) {
+            const float4 h = y.hi[base + begin + lane + 32 * i];
+            const float4 tp = y.tf[__float_as_int(h.w)];   // (c12, c6, shift, floor2)
+            const float2 dx = __fadd2_rn(make_float2(h.x, h.x), nsx),
+                         dy = __fadd2_rn(make_float2(h.y, h.y), nsy),
+                         dz = __fadd2_rn(make_float2(h.z, h.z), nsz);
+            const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+            float r0, r1;
+            asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(d2.x));
+            asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r1) : "f"(d2.y));
+            const float2 n1 = make_float2(r0, r1);
+            float2 n3 = __fmul2_rn(__fmul2_rn(n1, n1), n1);
+            if (MASK) {
+                const float2 m = make_float2(set_lt(d2.x, y.rc2f), set_lt(d2.y, y.rc2f));
+                n3 = __fmul2_rn(n3, m);
+                fe = __ffma2_rn(m, make_float2(tp.z, tp.z), fe);
+            } else {
+                fs += tp.z;
+            }
+            fe = __ffma2_rn(n3, __ffma2_rn(make_float2(tp.x, tp.x), n3, make_float2(-tp.y, -tp.y)),
+                            fe);
+            const float2 fp =
+                __fmul2_rn(__fmul2_rn(n1, n3),
+                           __ffma2_rn(make_float2(-2.f * tp.x, -2.f * tp.x), n3,
+                                      make_float2(tp.y, tp.y)));
+            gx = __ffma2_rn(fp, dx, gx);
+            gy = __ffma2_rn(fp, dy, gy);
+            gz = __ffma2_rn(fp, dz, gz);
+        }
+        v[0] += (double)fe.x + (double)fe.y;
+        if (!MASK) shift_sum += (double)fs;
+        v[1] -= 6.0 * (double)gx.x;
+        v[2] -= 6.0 * (double)gy.x;
+        v[3] -= 6.0 * (double)gz.x;
+        v[4] -= 6.0 * (double)gx.y;
+        v[5] -= 6.0 * (double)gy.y;
+        v[6] -= 6.0 * (double)gz.y;
+    }
+}
+
 // Sums of one pose over its bin list: v = (E, dE/dsite0 [3], dE/dsite1 [3]),
-// lane-partial (reduced by the caller).  FAR64 evaluates the far entries in
-// FP64 too (refinement).
+// lane-partial (reduced by the caller).  FAR64 evaluates every entry in FP64
+// with the correctly rounded reciprocal (refinement, and the FP64 mode whose
+// entries are all near); otherwise near entries in FP64 with the hardware
+// reciprocal seed + one Newton step (relative error <= 2^-46) and far entries
+// in packed FP32.
 template <bool FAR64>
 __device__ __forceinline__ void pose_sums(const PoseBatchSys &y, const RegionInfo &r,
                                           const double (&sd)[2][3], int lane, double (&v)[7]) {
@@ -51,7 +112,7 @@ __device__ __forceinline__ void pose_sums(const PoseBatchSys &y, const RegionInf
             const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
             if (d2 >= y.rc2) continue;
             const double s2 = d2 < fl ? fl : d2;
-            const double i2 = 1.0 / s2;
+            const double i2 = FAR64 ? 1.0 / s2 : rcp64_nr<1>(s2);
             const double i6 = i2 * i2 * i2;
             v[0] += fma(i6, fma(c12, i6, -c6), shift);
             if (d2 > fl) {
@@ -64,38 +125,16 @@ __device__ __forceinline__ void pose_sums(const PoseBatchSys &y, const RegionInf
         }
     }
     if (FAR64) return;
-    float sf[2][3];
-#pragma unroll
-    for (int s = 0; s < 2; ++s)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) sf[s][k] = (float)sd[s][k];
-    const int n_far = r.n_total - r.n_near;
-    const int mine = n_far > lane ? (n_far - lane + 31) / 32 : 0;   // this lane's far entries
-    for (int i0 = 0; i0 < mine; i0 += 16) {
-        float fv[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        const int i1 = min(i0 + 16, mine);
-        for (int i = i0; i < i1; ++i) {
-            const float4 h = y.hi[r.off + r.n_near + lane + 32 * i];
-            const float4 tp = y.tf[__float_as_int(h.w)];   // (c12, c6, shift, floor2)
-#pragma unroll
-            for (int s = 0; s < 2; ++s) {
-                const float dx = sf[s][0] - h.x, dy = sf[s][1] - h.y, dz = sf[s][2] - h.z;
-                const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                float n1;
-                asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(n1) : "f"(d2));
-                const float m = d2 < y.rc2f ? 1.f : 0.f;
-                const float n3 = n1 * n1 * n1 * m;
-                fv[0] += fmaf(n3, fmaf(tp.x, n3, -tp.y), m * tp.z);
-                // far pairs lie beyond r_split: no contact floor
-                const float w = (n1 * n3) * fmaf(-12.f * tp.x, n3, 6.f * tp.y);
-                fv[1 + 3 * s] = fmaf(w, dx, fv[1 + 3 * s]);
-                fv[2 + 3 * s] = fmaf(w, dy, fv[2 + 3 * s]);
-                fv[3 + 3 * s] = fmaf(w, dz, fv[3 + 3 * s]);
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < 7; ++k) v[k] += (double)fv[k];
-    }
+    // far entries lie beyond r_split of every site: no contact floor
+    const float2 nsx = make_float2(-(float)sd[0][0], -(float)sd[1][0]),
+                 nsy = make_float2(-(float)sd[0][1], -(float)sd[1][1]),
+                 nsz = make_float2(-(float)sd[0][2], -(float)sd[1][2]);
+    double shift_sum = 0.0;
+    far_lane_sums<false>(y, r.off, r.n_near, r.n_near + r.n_inner, lane, nsx, nsy, nsz, v,
+                         shift_sum);
+    far_lane_sums<true>(y, r.off, r.n_near + r.n_inner, r.n_total, lane, nsx, nsy, nsz, v,
+                        shift_sum);
+    v[0] += 2.0 * shift_sum;
 }
 
 __device__ __forceinline__ void warp_reduce7(double (&v)[7]) {
@@ -105,6 +144,8 @@ __device__ __forceinline__ void warp_reduce7(double (&v)[7]) {
         for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
 }
 
+// MIXED = false: the FP64 mode (every entry near, evaluated as in refinement).
+template <bool MIXED>
 __global__ void __launch_bounds__(256) pose_batch_kernel(PoseBatchArgs a) {
     const int lane = threadIdx.x & 31;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -151,9 +192,9 @@ __global__ void __launch_bounds__(256) pose_batch_kernel(PoseBatchArgs a) {
             sd[s][2] = cz + off * u[2];
         }
         double v[7] = {0, 0, 0, 0, 0, 0, 0};
-        pose_sums<false>(y, r, sd, lane, v);
+        pose_sums<!MIXED>(y, r, sd, lane, v);
         warp_reduce7(v);
-        if (v[0] > a.band_lo && v[0] < a.band_hi) {   // warp-uniform: every lane holds the sum
+        if (MIXED && v[0] > a.band_lo && v[0] < a.band_hi) {   // warp-uniform: all lanes hold it
 #pragma unroll
             for (int k = 0; k < 7; ++k) v[k] = 0.0;
             pose_sums<true>(y, r, sd, lane, v);
@@ -241,7 +282,8 @@ int pose_warp_enqueue(System *sys, const RegionSet *rs, int n, const double *cen
     a.band_hi = band ? o.band_hi : 0.0;
     a.status = sys->d_status;
     const long long blocks = std::min<long long>(((long long)n + 7) / 8, 148LL * 16);
-    pose_batch_kernel<<<(int)blocks, 256, 0, st>>>(a);
+    if (o.mode == VEXT_MODE_MIXED) pose_batch_kernel<true><<<(int)blocks, 256, 0, st>>>(a);
+    else pose_batch_kernel<false><<<(int)blocks, 256, 0, st>>>(a);
     VEXT_CUDA(cudaGetLastError());
     return 0;
 }
@@ -333,7 +375,10 @@ extern "C" int vext_pose_batch_run(vext_pose_batch b, const double *centers, con
     a.band_hi = band ? b->opt.band_hi : 0.0;
     a.status = b->d_status;
     const long long blocks = std::min<long long>((b->n + 7) / 8, 148LL * 16);
-    pose_batch_kernel<<<(int)blocks, 256, 0, (cudaStream_t)stream>>>(a);
+    if (b->opt.mode == VEXT_MODE_MIXED)
+        pose_batch_kernel<true><<<(int)blocks, 256, 0, (cudaStream_t)stream>>>(a);
+    else
+        pose_batch_kernel<false><<<(int)blocks, 256, 0, (cudaStream_t)stream>>>(a);
     VEXT_CUDA(cudaGetLastError());
     return 0;
 }
