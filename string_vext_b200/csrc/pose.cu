@@ -461,7 +461,7 @@ int pose_enqueue(System *sys, int n, const double *centers, const double *quats,
     const int n_bins = rs->n_regions;
     // Fewer than 64 poses per bin on average: the binned pipeline would give
     // most of its per-bin CTAs a handful of poses for a whole list each; one
-    // warp per pose is faster there (String paths, small batches).
+    // to eight warps per pose are faster there (String paths, small batches).
     if ((long long)n < 64LL * n_bins)
         return pose_warp_enqueue(sys, rs, n, centers, quats, o,
                                  energy ? energy : nullptr, gc, gq, gu, st);

@@ -2,9 +2,9 @@
 // the String paths of a batch of frameworks x guests (each path a few dozen
 // images), evaluated every iteration.
 //
-// One warp per pose.  The pose's center is wrapped into its system's cell and
-// binned (the bin lists of system.cu, built at creation); the 32 lanes stride
-// over the bin's list: near entries in FP64 from hi + lo with the contact
+// One to eight warps per pose (more for small batches).  The pose's center is
+// wrapped into its system's cell and binned (the bin lists of system.cu, built
+// at creation); the lanes stride over the bin's list: near entries in FP64 from hi + lo with the contact
 // floor, far entries in packed FP32x2 (the two sites in the two lanes;
 // reciprocal of d^2 per pair, cubed) with per-lane FP32 partials flushed into
 // FP64 every 16 entries.  The seven sums
@@ -31,9 +31,10 @@ struct PoseBatchArgs {
     double *energy, *gc, *gq, *gu;
     double band_lo, band_hi;
     int *status;
+    int wpp;                    // warps per pose (set at launch)
 };
 
-// This lane's far entries begin + lane + 32 i < end of one pose, the two
+// This lane's far entries begin + lane + stride i < end of one pose, the two
 // sites in the two lanes of the packed FP32x2 instructions (pose.cu's far loop):
 // d = x - r_s, n1 = hardware reciprocal of d2, n3 = n1^3, e = n3 (c12 n3 - c6),
 // fp = (n1 n3)(c6 - 2 c12 n3), dE/dsite += -6 fp d.  MASK = false for inner
@@ -42,16 +43,17 @@ struct PoseBatchArgs {
 // FP64 sums every 16 entries.
 template <bool MASK>
 __device__ __forceinline__ void far_lane_sums(const PoseBatchSys &y, long long base, int begin,
-                                              int end, int lane, float2 nsx, float2 nsy,
-                                              float2 nsz, double (&v)[7], double &shift_sum) {
-    const int mine = end - begin > lane ? (end - begin - lane + 31) / 32 : 0;
+                                              int end, int lane, int stride, float2 nsx,
+                                              float2 nsy, float2 nsz, double (&v)[7],
+                                              double &shift_sum) {
+    const int mine = end - begin > lane ? (end - begin - lane + stride - 1) / stride : 0;
 #pragma unroll 1
     for (int i0 = 0; i0 < mine; i0 += 16) {
         float2 fe = make_float2(0.f, 0.f), gx = fe, gy = fe, gz = fe;
         float fs = 0.f;
         const int i1 = min(i0 + 16, mine);
         for (int i = i0; i < i1; ++i) {
-            const float4 h = y.hi[base + begin + lane + 32 * i];
+            const float4 h = y.hi[base + begin + lane + (long long)stride * i];
             const float4 tp = y.tf[__float_as_int(h.w)];   // (c12, c6, shift, floor2)
             const float2 dx = __fadd2_rn(make_float2(h.x, h.x), nsx),
                          dy = __fadd2_rn(make_float2(h.y, h.y), nsy),
@@ -91,15 +93,16 @@ __device__ __forceinline__ void far_lane_sums(const PoseBatchSys &y, long long b
 }
 
 // Sums of one pose over its bin list: v = (E, dE/dsite0 [3], dE/dsite1 [3]),
-// lane-partial (reduced by the caller).  FAR64 evaluates every entry in FP64
+// partial over the entries lane, lane + stride, ... (reduced by the caller).  FAR64 evaluates every entry in FP64
 // with the correctly rounded reciprocal (refinement, and the FP64 mode whose
 // entries are all near); otherwise near entries in FP64 with the hardware
 // reciprocal seed + one Newton step (relative error <= 2^-46) and far entries
 // in packed FP32.
 template <bool FAR64>
 __device__ __forceinline__ void pose_sums(const PoseBatchSys &y, const RegionInfo &r,
-                                          const double (&sd)[2][3], int lane, double (&v)[7]) {
-    for (int e = lane; e < (FAR64 ? r.n_total : r.n_near); e += 32) {
+                                          const double (&sd)[2][3], int lane, int stride,
+                                          double (&v)[7]) {
+    for (int e = lane; e < (FAR64 ? r.n_total : r.n_near); e += stride) {
         const float4 h = y.hi[r.off + e], l = y.lo[r.off + e];
         const double x = (double)h.x + (double)l.x, yy = (double)h.y + (double)l.y,
                      z = (double)h.z + (double)l.z;
@@ -130,10 +133,10 @@ __device__ __forceinline__ void pose_sums(const PoseBatchSys &y, const RegionInf
                  nsy = make_float2(-(float)sd[0][1], -(float)sd[1][1]),
                  nsz = make_float2(-(float)sd[0][2], -(float)sd[1][2]);
     double shift_sum = 0.0;
-    far_lane_sums<false>(y, r.off, r.n_near, r.n_near + r.n_inner, lane, nsx, nsy, nsz, v,
-                         shift_sum);
-    far_lane_sums<true>(y, r.off, r.n_near + r.n_inner, r.n_total, lane, nsx, nsy, nsz, v,
-                        shift_sum);
+    far_lane_sums<false>(y, r.off, r.n_near, r.n_near + r.n_inner, lane, stride, nsx, nsy, nsz,
+                         v, shift_sum);
+    far_lane_sums<true>(y, r.off, r.n_near + r.n_inner, r.n_total, lane, stride, nsx, nsy, nsz,
+                        v, shift_sum);
     v[0] += 2.0 * shift_sum;
 }
 
@@ -144,13 +147,20 @@ __device__ __forceinline__ void warp_reduce7(double (&v)[7]) {
         for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
 }
 
-// MIXED = false: the FP64 mode (every entry near, evaluated as in refinement).
+// a.wpp warps (1, 2, 4 or 8) share a pose, its lanes striding over the bin
+// list together, so that small batches (a String path) still fill the GPU;
+// the warps' sums are added in shared memory in a fixed order.  MIXED = false:
+// the FP64 mode (every entry near, evaluated as in refinement).
 template <bool MIXED>
 __global__ void __launch_bounds__(256) pose_batch_kernel(PoseBatchArgs a) {
-    const int lane = threadIdx.x & 31;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < a.n;
-         p += nwarps) {
+    __shared__ double part[8][7];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int W = a.wpp, per_cta = 8 / W, sub = warp % W;
+    const long long groups = (a.n + per_cta - 1) / per_cta;
+    for (long long grp = blockIdx.x; grp < groups; grp += gridDim.x) {   // uniform per CTA
+        const long long p0 = grp * per_cta + warp / W;
+        const bool live = p0 < a.n;
+        const long long p = live ? p0 : a.n - 1;   // idle warps repeat the last pose, unwritten
         // system of pose p: offsets[k] <= p < offsets[k + 1]
         int lo = 0, hi = a.n_systems - 1;
         while (lo < hi) {
@@ -192,15 +202,30 @@ __global__ void __launch_bounds__(256) pose_batch_kernel(PoseBatchArgs a) {
             sd[s][2] = cz + off * u[2];
         }
         double v[7] = {0, 0, 0, 0, 0, 0, 0};
-        pose_sums<!MIXED>(y, r, sd, lane, v);
+        pose_sums<!MIXED>(y, r, sd, lane + 32 * sub, 32 * W, v);
         warp_reduce7(v);
+        if (W > 1) {   // (W is a launch argument: uniform over the CTA)
+            if (lane == 0)
+#pragma unroll
+                for (int k = 0; k < 7; ++k) part[warp][k] = v[k];
+            __syncthreads();
+            const int w0 = warp - sub;
+#pragma unroll
+            for (int k = 0; k < 7; ++k) {
+                double t = part[w0][k];
+                for (int j = 1; j < W; ++j) t += part[w0 + j][k];
+                v[k] = t;
+            }
+            __syncthreads();
+        }
+        if (sub != 0) continue;
         if (MIXED && v[0] > a.band_lo && v[0] < a.band_hi) {   // warp-uniform: all lanes hold it
 #pragma unroll
             for (int k = 0; k < 7; ++k) v[k] = 0.0;
-            pose_sums<true>(y, r, sd, lane, v);
+            pose_sums<true>(y, r, sd, lane, 32, v);
             warp_reduce7(v);
         }
-        if (lane == 0) {
+        if (live && lane == 0) {
             if (a.energy) a.energy[p] = v[0];
             double gu[3];
 #pragma unroll
@@ -225,6 +250,25 @@ __global__ void __launch_bounds__(256) pose_batch_kernel(PoseBatchArgs a) {
             }
         }
     }
+}
+
+// Warps per pose: the smallest power of two up to 8 that gives about 16
+// resident warps per SM (148 SMs), so small batches spread each pose's list
+// over several warps.
+static int warps_per_pose(long long n) {
+    int w = 1;
+    while (w < 8 && n * (2 * w) <= 148LL * 16) w *= 2;
+    return w;
+}
+
+static int pose_batch_launch(PoseBatchArgs a, bool mixed, cudaStream_t st) {
+    a.wpp = warps_per_pose(a.n);
+    const long long groups = (a.n + 8 / a.wpp - 1) / (8 / a.wpp);
+    const int blocks = (int)std::min<long long>(groups, 148LL * 16);
+    if (mixed) pose_batch_kernel<true><<<blocks, 256, 0, st>>>(a);
+    else pose_batch_kernel<false><<<blocks, 256, 0, st>>>(a);
+    VEXT_CUDA(cudaGetLastError());
+    return 0;
 }
 
 static PoseBatchSys describe(const System *sys, const RegionSet *rs) {
@@ -281,11 +325,7 @@ int pose_warp_enqueue(System *sys, const RegionSet *rs, int n, const double *cen
     a.band_lo = band ? o.band_lo : 0.0;
     a.band_hi = band ? o.band_hi : 0.0;
     a.status = sys->d_status;
-    const long long blocks = std::min<long long>(((long long)n + 7) / 8, 148LL * 16);
-    if (o.mode == VEXT_MODE_MIXED) pose_batch_kernel<true><<<(int)blocks, 256, 0, st>>>(a);
-    else pose_batch_kernel<false><<<(int)blocks, 256, 0, st>>>(a);
-    VEXT_CUDA(cudaGetLastError());
-    return 0;
+    return pose_batch_launch(a, o.mode == VEXT_MODE_MIXED, st);
 }
 
 }  // namespace vext
@@ -374,13 +414,7 @@ extern "C" int vext_pose_batch_run(vext_pose_batch b, const double *centers, con
     a.band_lo = band ? b->opt.band_lo : 0.0;
     a.band_hi = band ? b->opt.band_hi : 0.0;
     a.status = b->d_status;
-    const long long blocks = std::min<long long>((b->n + 7) / 8, 148LL * 16);
-    if (b->opt.mode == VEXT_MODE_MIXED)
-        pose_batch_kernel<true><<<(int)blocks, 256, 0, (cudaStream_t)stream>>>(a);
-    else
-        pose_batch_kernel<false><<<(int)blocks, 256, 0, (cudaStream_t)stream>>>(a);
-    VEXT_CUDA(cudaGetLastError());
-    return 0;
+    return pose_batch_launch(a, b->opt.mode == VEXT_MODE_MIXED, (cudaStream_t)stream);
 }
 
 extern "C" int vext_pose_batch_status(vext_pose_batch b) {

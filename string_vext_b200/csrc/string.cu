@@ -28,9 +28,10 @@
 //      (legacy_policy.h:9-12, RC_main.cu:1853-1854); on convergence the loop
 //      stops before the copy;
 //   8. s0 = (s2 positions, smoothed angles wrapped into [0, 2 pi]) (copy2s0).
-// Steps 2-8 run in two single-CTA kernels; the two pose evaluations are the
-// only heavy work.  One iteration is captured in a CUDA graph and replayed;
-// the host reads the stop flag only at check iterations.
+// Steps 2-8 run in two single-CTA kernels (one thread per image); the two
+// pose evaluations are the only heavy work.  One iteration is captured in a
+// CUDA graph and replayed; the host reads the stop flag only at check
+// iterations.
 #include <cmath>
 #include <vector>
 
@@ -75,11 +76,18 @@ __global__ void string_to_pose_kernel(StringArgs a) {
         pose_of(a, a.s0 + 6 * i, a.centers + 3 * i, a.quats + 4 * i);
 }
 
-// Steps 2-4 (and the pose of s2).  One CTA.
-__global__ void string_step_kernel(StringArgs a) {
-    if (a.flags[0]) return;   // converged earlier
-    const int n = a.n;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+// Steps 2-4 (and the pose of s2).  One CTA, thread i = image i (n <= 1024 =
+// blockDim): the step in registers, end fixing and segment lengths through
+// shared memory, the running sum of the lengths by one thread in image order.
+__global__ void __launch_bounds__(1024) string_step_kernel(StringArgs a) {
+    __shared__ double ax[1024];       // axis coordinate of every stepped image (before fixing)
+    __shared__ double cum[1024];      // segment lengths, then their running sums
+    __shared__ double cart[3][1024];  // Cartesian positions of the fixed images
+    __shared__ double pre0[6];        // image 0 before fixing
+    if (a.flags[0]) return;   // converged earlier (uniform over the CTA)
+    const int n = a.n, d = a.axis, i = threadIdx.x;
+    double o[6];
+    if (i < n) {
         const double *s = a.s0 + 6 * i;
         double g[6];
         // dE/dfrac_k = sum_j H[k][j] dE/dcart_j
@@ -95,72 +103,82 @@ __global__ void string_step_kernel(StringArgs a) {
         for (int k = 0; k < 6; ++k) g[k] = trunc_r(g[k], a.rounding);
         const double lt = trunc_r(sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]), a.rounding);
         const double lr = trunc_r(sqrt(g[3] * g[3] + g[4] * g[4] + g[5] * g[5]), a.rounding);
-        double *o = a.s1 + 6 * i;
         for (int k = 0; k < 3; ++k)
             o[k] = lt < a.hf ? s[k] - a.hf * g[k] : s[k] - a.hf * trunc_r(g[k] / lt, a.rounding);
         for (int k = 3; k < 6; ++k)
             o[k] = lr < a.ha ? s[k] - a.ha * g[k] : s[k] - a.ha * trunc_r(g[k] / lr, a.rounding);
+        // the values before fixing (s2), read by the images that copy them
+        for (int k = 0; k < 6; ++k) a.s2[6 * i + k] = o[k];
+        ax[i] = o[d];
+        if (i == 0)
+            for (int k = 0; k < 6; ++k) pre0[k] = o[k];
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        // end fixing; interior replacements read the values before fixing
-        // (s2 holds that copy)
-        for (int k = 0; k < 6 * n; ++k) a.s2[k] = a.s1[k];
-        const int d = a.axis;
-        a.s1[d] = a.s0[d];
-        a.s1[6 * (n - 1) + d] = a.s0[6 * (n - 1) + d];
-        for (int k = 0; k < 6; ++k)
-            if (k != d) a.s1[6 * (n - 1) + k] = a.s2[k];
-        for (int i = 1; i < n - 1; ++i) {
-            const double v = a.s2[6 * i + d];
+    if (i < n) {
+        // end fixing: image 0 keeps its axis coordinate; the last image keeps
+        // its axis coordinate and takes the other five from image 0; an
+        // interior image outside [0, 1] along the axis copies the nearest
+        // image inside (values before fixing)
+        if (i == 0) {
+            o[d] = a.s0[d];
+        } else if (i == n - 1) {
+            for (int k = 0; k < 6; ++k) o[k] = k == d ? a.s0[6 * (n - 1) + d] : pre0[k];
+        } else {
+            const double v = ax[i];
             int src = -1;
             if (v < 0) {
                 for (int ii = i + 1; ii < n; ++ii)
-                    if (a.s2[6 * ii + d] > 0) {
+                    if (ax[ii] > 0) {
                         src = ii;
                         break;
                     }
             } else if (v > 1) {
                 for (int ii = i - 1; ii >= 0; --ii)
-                    if (a.s2[6 * ii + d] < 1) {
+                    if (ax[ii] < 1) {
                         src = ii;
                         break;
                     }
             }
             if (src >= 0)
-                for (int k = 0; k < 6; ++k) a.s1[6 * i + k] = a.s2[6 * src + k];
+                for (int k = 0; k < 6; ++k) o[k] = a.s2[6 * src + k];
         }
-        // Cartesian segment lengths and their running sum
-        double px = 0, py = 0, pz = 0, cum = 0;
-        for (int i = 0; i < n; ++i) {
-            double x, y, z;
-            frac_to_cart(a.H, a.s1[6 * i], a.s1[6 * i + 1], a.s1[6 * i + 2], x, y, z);
-            if (i) cum += sqrt((x - px) * (x - px) + (y - py) * (y - py) + (z - pz) * (z - pz));
-            a.lengths[i] = cum;
-            px = x;
-            py = y;
-            pz = z;
+        for (int k = 0; k < 6; ++k) a.s1[6 * i + k] = o[k];
+        frac_to_cart(a.H, o[0], o[1], o[2], cart[0][i], cart[1][i], cart[2][i]);
+    }
+    __syncthreads();
+    if (i < n && i > 0) {
+        const double dx = cart[0][i] - cart[0][i - 1], dy = cart[1][i] - cart[1][i - 1],
+                     dz = cart[2][i] - cart[2][i - 1];
+        cum[i] = sqrt(dx * dx + dy * dy + dz * dz);
+    }
+    __syncthreads();
+    if (i == 0) {   // running sum in image order
+        double c = 0;
+        cum[0] = 0;
+        for (int k = 1; k < n; ++k) {
+            c += cum[k];
+            cum[k] = c;
         }
     }
     __syncthreads();
-    const double L = a.lengths[n - 1];
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    if (i < n) {   // (s2 is read above only, three barriers back: rewrite it now)
+        const double L = cum[n - 1];
         const double t = (double)i / (n - 1);
         // segment ii with cum[ii]/L <= t <= cum[ii+1]/L (binary search)
         int lo = 0, hi = n - 2;
         while (lo < hi) {
             const int mid = (lo + hi + 1) / 2;
-            if (a.lengths[mid] / L <= t) lo = mid;
+            if (cum[mid] / L <= t) lo = mid;
             else hi = mid - 1;
         }
         const int ii = lo;
-        const double l0 = a.lengths[ii] / L, l1 = a.lengths[ii + 1] / L;
-        double *o = a.s2 + 6 * i;
+        const double l0 = cum[ii] / L, l1 = cum[ii + 1] / L;
+        double *out = a.s2 + 6 * i;
         const double *p0 = a.s1 + 6 * ii, *p1 = a.s1 + 6 * (ii + 1);
         for (int k = 0; k < 3; ++k)
-            o[k] = l1 > l0 ? p0[k] + (t - l0) * ((p1[k] - p0[k]) / (l1 - l0)) : p0[k];
-        for (int k = 3; k < 6; ++k) o[k] = a.s1[6 * i + k];
-        pose_of(a, o, a.centers2 + 3 * i, a.quats2 + 4 * i);
+            out[k] = l1 > l0 ? p0[k] + (t - l0) * ((p1[k] - p0[k]) / (l1 - l0)) : p0[k];
+        for (int k = 3; k < 6; ++k) out[k] = o[k];
+        pose_of(a, out, a.centers2 + 3 * i, a.quats2 + 4 * i);
     }
 }
 
@@ -196,7 +214,7 @@ __global__ void string_finish_kernel(StringArgs a, int check) {
     __syncthreads();
     if (threadIdx.x == 0) {
         double t = 0, r = 0;
-        for (int k = 0; k < (int)blockDim.x; ++k) {
+        for (int k = 0; k < min(n, (int)blockDim.x); ++k) {   // (the other threads hold 0)
             t += red[0][k];
             r += red[1][k];
         }

@@ -49,6 +49,24 @@ def test_iterations_match_cpu_restatement(n_iter):
     np.testing.assert_allclose(e_gpu, string_oracle.pose_energy(case, gpu), rtol=1e-10, atol=1e-8)
 
 
+@pytest.mark.parametrize("n_images", [64, 45])
+def test_end_fixing_matches_cpu_restatement(n_images):
+    """Interior images pushed outside [0, 1] along the transport axis copy the
+    nearest image inside (values before fixing); the ends keep their axis
+    coordinate: one iteration against the CPU restatement, also for an image
+    count that leaves a warp partly idle."""
+    case, s = path_config4()
+    s = s[np.linspace(0, len(s) - 1, n_images).round().astype(int)].copy()
+    s[1:4, 2] = [-0.05, -0.03, -0.01]
+    s[-4:-1, 2] = [1.01, 1.03, 1.05]
+    with VextSystem(case) as system:
+        gpu, _, res = run_string(system, s, mode=FP64, direction=3, max_iterations=1)
+    ref, _, _, _ = string_oracle.iteration(case, s.copy(), direction=3)
+    assert res["iterations"] == 1
+    np.testing.assert_allclose(gpu[:, :3], ref[:, :3], rtol=0, atol=1e-10)
+    np.testing.assert_allclose(gpu[:, 3:], ref[:, 3:], rtol=0, atol=1e-9)
+
+
 def test_analytic_step_agrees_with_reference_fd_forces():
     """One step with the reference's one-sided forces (h = 1e-4 frac, 1 deg)
     versus the analytic forces: the positions move alike."""
