@@ -285,3 +285,18 @@ def test_host_entry_into_page_locked_buffers():
         np.testing.assert_array_equal(sg.numpy().reshape(shape + (6,)), ref_g)
         for big in (be, bg):
             assert (big[:pad] == -7.0).all() and (big[-pad:] == -7.0).all()
+
+
+@pytest.mark.parametrize("mode", [FP64, _lib.VEXT_MODE_FP64_PLAIN])
+def test_host_entry_fp64_modes(mode):
+    """The host entry in the FP64 modes (staged copies) returns the device
+    entry's float32 energy and gradient bit for bit."""
+    case = synth.skewed_field()
+    size = 5
+    _, axes = regular_pose_grid(size, 64)
+    axes = normalized_directors(axes)
+    with VextSystem(case) as system:
+        ref_e, ref_g = run_device(system, size, axes, mode)
+        e, g = system.field_adjoint(size, axes, mode=mode)
+        np.testing.assert_array_equal(e, ref_e)
+        np.testing.assert_array_equal(g, ref_g)

@@ -154,3 +154,26 @@ def test_string_path_and_random_batch():
             assert (np.abs(e - e64) / np.maximum(np.abs(e64), 1))[~neg].max(initial=0) < 1e-6
             ref = oracle.pose_energy_grad(case, cart[:64], director(quat[:64]))[0]
             np.testing.assert_allclose(e64[:64], ref, rtol=1e-10, atol=1e-8)
+
+
+@pytest.mark.parametrize("n", [1, 7, 301, 1000])
+def test_small_batches_of_any_size(small, n):
+    """Small batches take the kernel that spreads each pose's bin list over one
+    to eight warps (8 for n <= 296, 4 for n = 301 with one idle warp group in
+    the last CTA, 2 for n = 1000): mixed within the bar of the FP64 oracle,
+    FP64 to 1e-10."""
+    case, system = small
+    c, q = random_poses(case, n, 100 + n)
+    re, rgc, rgu = oracle.pose_energy_grad(case, c, director(q))
+    e, gc, gq, gu = system.pose_energy_grad(c, q, mode=FP64)
+    np.testing.assert_allclose(e, re, rtol=1e-10, atol=1e-8)
+    scale = np.maximum(np.abs(rgc).max(axis=1, keepdims=True), 1.0)
+    assert (np.abs(gc - rgc) / scale).max() < 1e-9
+    e, gc, gq, gu = system.pose_energy_grad(c, q, mode=MIXED)
+    neg = re <= 0
+    if neg.any():
+        assert np.abs(e - re)[neg].max() < 1e-4
+    assert (np.abs(e - re) / np.maximum(np.abs(re), 1))[~neg].max() < 1e-6
+    assert (np.abs(gc - rgc) / scale).max() < 1e-5
+    scale_u = np.maximum(np.abs(rgu).max(axis=1, keepdims=True), 1.0)
+    assert (np.abs(gu - rgu) / scale_u).max() < 1e-5
