@@ -4,14 +4,15 @@
 //
 // One to eight warps per pose (more for small batches).  The pose's center is
 // wrapped into its system's cell and binned (the bin lists of system.cu, built
-// at creation); the lanes stride over the bin's list: near entries in FP64 from hi + lo with the contact
-// floor, far entries in packed FP32x2 (the two sites in the two lanes;
-// reciprocal of d^2 per pair, cubed) with per-lane FP32 partials flushed into
-// FP64 every 16 entries.  The seven sums
-// (E, dE/dsite for both sites) are reduced over the warp; a pose whose energy
-// falls in the refinement band is recomputed entirely in FP64 by the same
-// warp.  Outputs as vext_pose_energy_grad: E, dE/dcenter, tangent dE/dq,
-// dE/du.  Pair term and forces as in pose.cu.
+// at creation); the lanes stride over the bin's list: near entries in FP64
+// from hi + lo with the contact floor, far entries in packed FP32x2 (the two
+// sites in the two lanes; reciprocal of d^2 per pair, cubed) with per-lane
+// FP32 partials flushed into FP64 every 16 entries.  The seven sums (E,
+// dE/dsite for both sites) are reduced over the warp, then over the pose's
+// warps in shared memory; a pose whose energy falls in the refinement band is
+// recomputed entirely in FP64 by its first warp.  Outputs as
+// vext_pose_energy_grad: E, dE/dcenter, tangent dE/dq, dE/du.  Pair term and
+// forces as in pose.cu.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
