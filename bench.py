@@ -10,11 +10,13 @@ kernel), region lists and outputs resident in HBM.
 Our arm prints one JSON line with: value (poses/s over all ranks, device time
 from CUDA events, max over ranks), e2e (the public host C-ABI call
 vext_field_adjoint: directors up, float32 energy + gradient down into pinned
-host memory), roofline of the fused pair kernel against the measured FP32
+host memory, which the kernels write over PCIe during the pair work), roofline of the fused pair kernel against the measured FP32
 FFMA peak of this GPU, the forward-only field (list build + pair kernels +
 epilogue, with the far kernel's roofline), the plain and tiled FP64 GPU
 kernels and the error of the mixed result against FP64, the random-pose
-forward+adjoint path, the 100-field batches, clocks sampled during the timed
+forward+adjoint path and its error against its FP64 mode, the precision
+study, the GPU String update, the 100-field batches and 100 String paths,
+clocks sampled during the timed
 region, and a CPU baseline (the reference kernel compiled from its source,
 driven by the restated reference driver, on a bounded sample of the field).
 
