@@ -15,7 +15,9 @@ FFMA peak of this GPU, the forward-only field (list build + pair kernels +
 epilogue, with the far kernel's roofline), the plain and tiled FP64 GPU
 kernels and the error of the mixed result against FP64, the random-pose
 forward+adjoint path and its error against its FP64 mode, the precision
-study, the GPU String update, the 100-field batches and 100 String paths,
+study, the GPU String update, the drop-in mode (the reference's driver calling
+this library's evaluate_reused_neighbors), the 100-field batches and 100
+String paths,
 clocks sampled during the timed
 region, and a CPU baseline (the reference kernel compiled from its source,
 driven by the restated reference driver, on a bounded sample of the field).
@@ -501,6 +503,7 @@ def secondary_measurements(args, system, case, size, axes, poses, pairs, far_pai
     del cart, q, e, gc, gq, e64p, gc64, gq64
     out["precision_study"] = precision_study(device)
     out["string_update"] = bench_string_update()
+    out["dropin"] = bench_dropin(case, size, axes)
     if not args.no_batch:
         out["batch"] = bench_batch(args, size, axes, device, stream, adjoint=False)
         out["batch_fwd_adjoint"] = bench_batch(args, size, axes, device, stream, adjoint=True)
@@ -561,6 +564,36 @@ def bench_string_update():
             "ms_per_iteration": 1e3 * wall / max(res["iterations"], 1),
             "workload": "config-4 path, 64 images, 200 iterations, host wall time of "
                         "vext_string_run (graph-replayed iterations)"}
+
+
+def bench_dropin(case, size, axes):
+    """The drop-in mode: the reference's own driver (restated in
+    string_vext_b200/native.py: host kd-tree query and CSR per 512-center
+    batch, one process) calling this library's evaluate_reused_neighbors, on
+    the strided center sample of cpu_baseline_single_core.  Poses/s with the
+    host query and for the library calls alone (host buffers in and out)."""
+    from string_vext_b200.native import NativeReusePotential
+    from string_vext_b200.orientation import regular_pose_grid
+    centers, _ = regular_pose_grid(size, len(axes))
+    n_sample = int(min(len(centers), max(512, CPU_CENTERS_PER_CORE_S * 5.0)))
+    stride = max(1, len(centers) // n_sample)
+    sample = centers[::stride][:n_sample]
+    pot = NativeReusePotential(case)
+    pot.evaluate(sample[:512], axes)          # device buffers and context
+    pot.query_seconds = pot.compute_seconds = 0.0
+    t0 = time.perf_counter()
+    pot.evaluate(sample, axes)
+    wall = time.perf_counter() - t0
+    poses = len(sample) * len(axes)
+    return {"value": poses / wall, "unit": "poses/s",
+            "library_calls_only": poses / pot.compute_seconds,
+            "query_share": pot.query_seconds / wall,
+            "sample": f"{len(sample)} of {len(centers)} grid centers (stride {stride}) x "
+                      f"{len(axes)} directors, one process; {wall:.2f} s, kd-tree query "
+                      f"{pot.query_seconds:.2f} s, library calls {pot.compute_seconds:.2f} s",
+            "path": "reference driver (kd-tree + CSR on the host) -> "
+                    "evaluate_reused_neighbors of this library (FP64, bit-identical to the "
+                    "reference kernel)"}
 
 
 def bench_string_batch(device, stream):
