@@ -2,7 +2,7 @@
 // random pose batches, the torch autograd path).
 //
 // Poses are wrapped into the cell (FP64) and binned on a fractional grid of
-// ~2 A bins; every bin is a region with its own list (built once per system,
+// ~1.5 A bins; every bin is a region with its own list (built once per system,
 // system.cu).  One CTA = one work item (a bin and up to kPoseThreads of its
 // poses, one pose per thread).  Pair terms are recomputed, never stored:
 //   E   = sum  c12 i6^2 - c6 i6 + shift                 (d2 < rc^2)

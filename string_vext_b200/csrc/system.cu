@@ -363,6 +363,9 @@ int get_field_regions(System *sys, int size, int cb, double r_split, RegionSet *
     return 0;
 }
 
+// Width (A, between lattice planes) of the pose bins.
+constexpr double kBinWidth = 1.5;
+
 int get_bin_regions(System *sys, double r_split, RegionSet **out, cudaStream_t stream) {
     for (RegionSet *rs : sys->sets)
         if (rs->size == 0 && rs->r_split == r_split) {
@@ -375,9 +378,9 @@ int get_bin_regions(System *sys, double r_split, RegionSet **out, cudaStream_t s
         }
     RegionSet *rs = new RegionSet();
     rs->r_split = r_split;
-    // Bins about 2 A wide between lattice planes.
+    // Bins about kBinWidth wide between lattice planes.
     for (int k = 0; k < 3; ++k)
-        rs->nb[k] = std::max(1, (int)std::ceil((1.0 / sys->einv[k]) / 2.0));
+        rs->nb[k] = std::max(1, (int)std::ceil((1.0 / sys->einv[k]) / kBinWidth));
     rs->n_ri = rs->nb[0];
     rs->n_rj = rs->nb[1];
     rs->n_rk = rs->nb[2];
