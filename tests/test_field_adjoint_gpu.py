@@ -300,3 +300,31 @@ def test_host_entry_fp64_modes(mode):
         e, g = system.field_adjoint(size, axes, mode=mode)
         np.testing.assert_array_equal(e, ref_e)
         np.testing.assert_array_equal(g, ref_g)
+
+
+def test_director_reversal_at_full_size():
+    """Two identical sites at +-o: reversing every director swaps the sites, so
+    on the full 60^3 x 64 field the energy and dE/dcenter are unchanged and the
+    tangent dE/du changes sign, within the mixed bar of each result (both
+    carry their own FP32 rounding: twice the bar)."""
+    case = synth.full_field()
+    size = 60
+    _, axes = regular_pose_grid(size, 64)
+    axes = normalized_directors(axes)
+    shape = (64, size, size, size)
+    with VextSystem(case) as system:
+        results = []
+        for a in (axes, -axes):
+            e = torch.empty(shape, dtype=torch.float32, device="cuda")
+            g = torch.empty(shape + (6,), dtype=torch.float32, device="cuda")
+            e64 = torch.empty(shape, dtype=torch.float64, device="cuda")
+            system.field_adjoint_device(size, np.ascontiguousarray(a), e, g, e64)
+            torch.cuda.synchronize()
+            results.append((e64, g))
+        (ea, ga), (eb, gb) = results
+        rel = ((ea - eb).abs() / ea.abs().clamp(min=1.0)).max().item()
+        assert rel < 2e-6, rel
+        scale = ga[..., :3].norm(dim=-1).clamp(min=1.0)
+        assert ((ga[..., :3] - gb[..., :3]).norm(dim=-1) / scale).max().item() < 2e-5
+        scale = ga[..., 3:].norm(dim=-1).clamp(min=1.0)
+        assert ((ga[..., 3:] + gb[..., 3:]).norm(dim=-1) / scale).max().item() < 2e-5
