@@ -276,6 +276,9 @@ def test_host_entry_into_page_locked_buffers():
             e, g = system.field_adjoint(size, axes)      # pageable numpy outputs
             np.testing.assert_array_equal(e, ref_e)
             np.testing.assert_array_equal(g, ref_g)
+            e, g = system.field_adjoint(size, axes, pinned=True)
+            np.testing.assert_array_equal(e, ref_e)
+            np.testing.assert_array_equal(g, ref_g)
         pad = 16
         be = torch.full((n + 2 * pad,), -7.0, dtype=torch.float32, pin_memory=True)
         bg = torch.full((6 * n + 2 * pad,), -7.0, dtype=torch.float32, pin_memory=True)
