@@ -240,7 +240,9 @@ __device__ __forceinline__ void pose_far(const float4 *hb, const float4 *stf, in
 // MIXED: near pairs take the FP64 reciprocal as a hardware seed + one Newton
 // step (relative error <= 2^-46) and far pairs the packed FP32 loop; otherwise
 // (the FP64 mode: every entry is near) the correctly rounded reciprocal.
-template <int NT, bool MIXED>
+// NEAR_IN: the host proved every near pair inside the cutoff (r_split + 2
+// (rho + max|offset|) < rc), so near pairs skip the cutoff test.
+template <int NT, bool MIXED, bool NEAR_IN>
 __global__ void __launch_bounds__(NT) pose_kernel(PoseArgs a) {
     const int item = blockIdx.x;
     if (item >= a.items[0]) return;   // uniform over the CTA
@@ -330,7 +332,7 @@ __global__ void __launch_bounds__(NT) pose_kernel(PoseArgs a) {
                     const double i2 = MIXED ? rcp64_nr<1>(s2) : __drcp_rn(s2);
                     const double i6 = i2 * i2 * i2;
                     const double en = fma(i6, fma(cc.x, i6, -cc.y), sh.x);
-                    const bool in = d2 < a.rc2;
+                    const bool in = NEAR_IN || d2 < a.rc2;
                     const double w = (in && d2 > sh.y) ? i2 * i6 * fma(a12, i6, a6) : 0.0;
                     E[q] += in ? en : 0.0;
                     F[q][0] = fma(w, dx, F[q][0]);
@@ -521,8 +523,13 @@ int pose_enqueue(System *sys, int n, const double *centers, const double *quats,
     pose_scatter_kernel<<<pb, 256, 0, st>>>(a);
     VEXT_CUDA(cudaGetLastError());
     const size_t smem = kStageBytes + (size_t)kCH * 4 * sizeof(double) + (size_t)a.n_types * 48;
-    auto kernel = o.mode == VEXT_MODE_MIXED ? pose_kernel<kPoseThreads, true>
-                                            : pose_kernel<kPoseThreads, false>;
+    double rho = 0;
+    for (const RegionInfo &r : rs->h_info) rho = std::max(rho, r.rho);
+    const bool near_in = o.mode == VEXT_MODE_MIXED &&
+                         r_split + 2.0 * (rho + sys->max_offset) + 1e-6 < sys->cutoff;
+    auto kernel = o.mode != VEXT_MODE_MIXED ? pose_kernel<kPoseThreads, false, false>
+                  : near_in                 ? pose_kernel<kPoseThreads, true, true>
+                                            : pose_kernel<kPoseThreads, true, false>;
     VEXT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kernel<<<max_items, kPoseThreads, smem, st>>>(a);
     VEXT_CUDA(cudaGetLastError());
