@@ -53,7 +53,7 @@ METRIC = "Vext pose evals/s at <=1e-4 K vs FP64, fwd+adjoint evals/s; % FP32 pea
 FAR_DRAM_BYTES_FULL_FIELD = 744_213_504 + 100_719_360
 # the same for one forward + adjoint batch_field_kernel launch on full_field,
 # from an ncu capture (--set full) of `bench.py --profile adjoint`.
-ADJ_DRAM_BYTES_FULL_FIELD = 423_897_344 + 352_798_720
+ADJ_DRAM_BYTES_FULL_FIELD = 805_613_568 + 368_731_648
 CPU_CENTERS_PER_CORE_S = 900.0   # reference driver throughput estimate used to size the sample
 
 

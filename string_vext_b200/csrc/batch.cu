@@ -432,14 +432,20 @@ static const BatchKernel kAdjointFlush16Kernels[] = {   // accuracy/speed study
 static const BatchKernel kAdjointFlush64Kernels[] = {   // accuracy/speed study
     {batch_field_kernel<16, 16, 2, 2, 7>, 256, "256x2 flush64"},
     {batch_field_kernel<16, 8, 4, 2, 7>, 128, "128x4 flush64"}};
+// 8-center regions x 64-director items (the same 512 poses per staged
+// entry): a smaller region radius, hence shorter near and shell lists
+static const BatchKernel kAdjointCb8Kernels[] = {
+    {batch_field_kernel<8, 16, 4, 3, 8>, 128, "8c 128x4/3 gsum"},
+    {batch_field_kernel<8, 16, 4, 2, 1>, 128, "8c 128x4"}};
 constexpr int kMaxCandidates = 12;
 
 #define VEXT_COUNT(t) (int)(sizeof t / sizeof t[0])
 
-// kind: 0 forward, 1 forward + adjoint (default: reciprocal of q, cubed),
+// kind: 0 forward, 1 forward + adjoint (reciprocal of q, cubed),
 // 2 with the reciprocal of q^3 and a Newton step, 3 the same without it,
 // 4 / 5 default with FP32 gradient partials over 16 / 64 entries (a whole
-// 128-entry chunk by default; the energy partials always cover 16)
+// 128-entry chunk by default; the energy partials always cover 16), 6 default
+// on 8-center regions with 64-director items
 static int batch_kernel_count(int kind) {
     switch (kind) {
     case 0: return VEXT_COUNT(kForwardKernels);
@@ -447,6 +453,7 @@ static int batch_kernel_count(int kind) {
     case 2: return VEXT_COUNT(kAdjointNewtonKernels);
     case 4: return VEXT_COUNT(kAdjointFlush16Kernels);
     case 5: return VEXT_COUNT(kAdjointFlush64Kernels);
+    case 6: return VEXT_COUNT(kAdjointCb8Kernels);
     default: return VEXT_COUNT(kAdjointRcp3Kernels);
     }
 }
@@ -458,8 +465,25 @@ static const BatchKernel &batch_kernel(int kind, int shape) {
     case 2: return kAdjointNewtonKernels[shape];
     case 4: return kAdjointFlush16Kernels[shape];
     case 5: return kAdjointFlush64Kernels[shape];
+    case 6: return kAdjointCb8Kernels[shape];
     default: return kAdjointRcp3Kernels[shape];
     }
+}
+
+// The kernel table of a batch: forward (0), the forward + adjoint studies
+// (2-5, selected by variant bits), forward + adjoint on 16-center regions
+// (1, centers_per_region 16 or 32) or, by default, on 8-center regions (6).
+static int batch_kind(const Options &o, bool adj) {
+    if (!adj) return 0;
+    if (o.variant & 32) return 2;
+    if (o.variant & 64) return 3;
+    if (o.variant & 128) return 4;
+    if (o.variant & 512) return 5;
+    return o.cb == 16 || o.cb == 32 ? 1 : 6;
+}
+
+int batch_item_directors(const Options &o, bool adj) {
+    return batch_kind(o, adj) == 6 ? 64 : 32;
 }
 
 }  // namespace vext
@@ -562,12 +586,7 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
     b->n_axes = n_axes;
     b->opt = resolve_options(opt);
     b->adj = gradients != nullptr;
-    b->kind = !b->adj                 ? 0
-              : (b->opt.variant & 32)  ? 2
-              : (b->opt.variant & 64)  ? 3
-              : (b->opt.variant & 128) ? 4
-              : (b->opt.variant & 512) ? 5
-                                       : 1;
+    b->kind = batch_kind(b->opt, b->adj);
     if (b->opt.mode != VEXT_MODE_MIXED)
         return fail(VEXT_ERR_ARGUMENT, "batched fields run in the mixed mode only");
     int dev = 0;
@@ -575,7 +594,8 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
     VEXT_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     VEXT_CUDA(cudaMalloc(&b->d_axes, sizeof(double) * 3 * n_axes));
     VEXT_CUDA(cudaMemcpy(b->d_axes, axes, sizeof(double) * 3 * n_axes, cudaMemcpyHostToDevice));
-    constexpr int kOB = 32;   // directors per item (both CTA shapes cover 32)
+    // regions of 16 centers x items of 32 directors, or 8 x 64 (kind 6)
+    const int kOB = batch_item_directors(b->opt, b->adj), cb = 512 / kOB;
     std::vector<BatchSys> hs(n_systems);
     std::vector<std::pair<long long, int4>> items;
     for (int k = 0; k < n_systems; ++k) {
@@ -585,7 +605,7 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
         std::unique_lock<std::mutex> lock(sys->lock, std::defer_lock);
         if (lock_systems) lock.lock();
         RegionSet *rs = nullptr;
-        VEXT_TRY(get_field_regions(sys, size, 16, b->opt.r_split, &rs, sys->stream));
+        VEXT_TRY(get_field_regions(sys, size, cb, b->opt.r_split, &rs, sys->stream));
         BatchSys &y = hs[k];
         y.H = sys->H;
         y.rc2 = sys->cutoff * sys->cutoff;

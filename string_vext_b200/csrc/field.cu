@@ -809,6 +809,12 @@ extern "C" int vext_field_device(vext_system h, int size, int n_axes, const doub
 
 namespace vext {
 
+// Cache key of the options that shape a batch (kernel table, pinned shape,
+// region size).
+static double batch_key(const Options &o) {
+    return o.variant + 65536.0 * o.batch_shape + 16777216.0 * o.cb;
+}
+
 static int field_adjoint_device(vext_system h, int size, int n_axes, const double *axes,
                                 const Options &o, const vext_options *opt, float *energy,
                                 float *gradient, double *energy_f64, double *gradient_f64,
@@ -831,7 +837,7 @@ static int field_adjoint_device(vext_system h, int size, int n_axes, const doubl
                           std::equal(axes, axes + 3 * n_axes, sys->adj_axes.begin()) &&
                           sys->adj_key[0] == o.r_split && sys->adj_key[1] == o.band_lo &&
                           sys->adj_key[2] == o.band_hi &&
-                          sys->adj_key[3] == o.variant + 65536.0 * o.batch_shape &&
+                          sys->adj_key[3] == batch_key(o) &&
                           sys->adj_energy64 == energy_f64;
         if (!same) {
             if (sys->adj_batch) vext_batch_destroy(sys->adj_batch);   // (host parts stay)
@@ -845,7 +851,7 @@ static int field_adjoint_device(vext_system h, int size, int n_axes, const doubl
             sys->adj_key[0] = o.r_split;
             sys->adj_key[1] = o.band_lo;
             sys->adj_key[2] = o.band_hi;
-            sys->adj_key[3] = o.variant + 65536.0 * o.batch_shape;
+            sys->adj_key[3] = batch_key(o);
             sys->adj_energy64 = energy_f64;
         }
         // other float32 outputs than the last call's: a stream-ordered update
@@ -949,27 +955,28 @@ extern "C" int vext_field_adjoint(vext_system h, int size, int n_axes, const dou
         }
     }
     if (o.mode == VEXT_MODE_MIXED) {
-        // pageable host outputs: one batch per 32-director block; block k's
-        // copy (on aux) overlaps block k + 1's pair work (on st)
+        // pageable host outputs: one batch per block of the batch's work-item
+        // directors (64 by default); block k's copy (on aux) overlaps block
+        // k + 1's pair work (on st)
         for (int k = 0; k < 3 * n_axes; ++k)
             if (!std::isfinite(axes[k])) return fail(VEXT_ERR_ARGUMENT, "non-finite director");
         const size_t S3 = (size_t)size * size * size;
-        const int parts = (n_axes + 31) / 32;
+        const int blk = batch_item_directors(o, true), parts = (n_axes + blk - 1) / blk;
         const bool same = (int)sys->host_parts.size() == parts && sys->host_size == size &&
                           sys->host_axes.size() == 3 * (size_t)n_axes &&
                           std::equal(axes, axes + 3 * n_axes, sys->host_axes.begin()) &&
                           sys->host_key[0] == o.r_split && sys->host_key[1] == o.band_lo &&
                           sys->host_key[2] == o.band_hi &&
-                          sys->host_key[3] == o.variant + 65536.0 * o.batch_shape &&
+                          sys->host_key[3] == batch_key(o) &&
                           sys->host_e == sys->d_f32 && sys->host_g == sys->d_g32;
         if (!same) {
             sys->drop_host_parts();
             for (int k = 0; k < parts; ++k) {
-                const int nk = std::min(32, n_axes - 32 * k);
-                float *ek = sys->d_f32 + 32 * (size_t)k * S3;
-                float *gk = sys->d_g32 + 6 * 32 * (size_t)k * S3;
+                const int nk = std::min(blk, n_axes - blk * k);
+                float *ek = sys->d_f32 + blk * (size_t)k * S3;
+                float *gk = sys->d_g32 + 6 * blk * (size_t)k * S3;
                 vext_batch b = nullptr;
-                VEXT_TRY(batch_build(1, &h, size, nk, axes + 3 * 32 * k, opt, &ek, &gk, nullptr,
+                VEXT_TRY(batch_build(1, &h, size, nk, axes + 3 * blk * k, opt, &ek, &gk, nullptr,
                                      false, &b));
                 sys->host_parts.push_back(b);
                 cudaEvent_t ev;
@@ -981,12 +988,13 @@ extern "C" int vext_field_adjoint(vext_system h, int size, int n_axes, const dou
             sys->host_key[0] = o.r_split;
             sys->host_key[1] = o.band_lo;
             sys->host_key[2] = o.band_hi;
-            sys->host_key[3] = o.variant + 65536.0 * o.batch_shape;
+            sys->host_key[3] = batch_key(o);
             sys->host_e = sys->d_f32;
             sys->host_g = sys->d_g32;
         }
         for (int k = 0; k < parts; ++k) {
-            const size_t first = 32 * (size_t)k * S3, count = std::min(32, n_axes - 32 * k) * S3;
+            const size_t first = blk * (size_t)k * S3,
+                         count = std::min(blk, n_axes - blk * k) * S3;
             VEXT_TRY(batch_replay(sys->host_parts[k], st));
             VEXT_CUDA(cudaEventRecord(sys->host_part_done[k], st));
             VEXT_CUDA(cudaStreamWaitEvent(sys->aux, sys->host_part_done[k], 0));

@@ -184,6 +184,10 @@ struct Options {
 };
 Options resolve_options(const vext_options *opt);
 
+// Directors per work item of a batch with these options (32 or 64; its
+// regions hold 512 / that many grid centers).
+int batch_item_directors(const Options &o, bool adjoint);
+
 // Pose pipeline (pose.cu): enqueue without host synchronisation, then check.
 int pose_enqueue(System *sys, int n, const double *centers, const double *quats,
                  const Options &o, double *energy, double *gc, double *gq, double *gu,

@@ -175,27 +175,36 @@ def test_adjoint_rejects_bad_arguments():
 def test_every_batch_shape_gives_identical_results(maker, size):
     """Each CTA shape the autotuner may pick (pinned with batch_shape) does the
     same per-director arithmetic in the same order: forward and forward +
-    adjoint outputs are bit-identical across shapes."""
+    adjoint outputs are bit-identical across the shapes of a kernel table
+    (forward + adjoint: 8-center regions by default, 16-center regions with
+    centers_per_region=16; the two tables' lists differ, so do their bits)."""
     case = maker()
     _, axes = regular_pose_grid(size, 64)
     axes = normalized_directors(axes)
     shape = (64, size, size, size)
     with VextSystem(case) as system:
-        ref_e, ref_g = run_device(system, size, axes, MIXED)
-        probe = VextBatch([system], size, axes,
-                          [torch.empty(shape, dtype=torch.float32, device="cuda")],
-                          gradients=[torch.empty(shape + (6,), dtype=torch.float32,
-                                                 device="cuda")])
-        n_adj = len({t["shape"] for t in probe.tuning()})
-        probe.close()
-        assert n_adj >= 5
-        for k in range(1, n_adj + 1):
+        for cb, min_shapes in ((0, 2), (16, 5)):
             e = torch.empty(shape, dtype=torch.float32, device="cuda")
             g = torch.empty(shape + (6,), dtype=torch.float32, device="cuda")
-            system.field_adjoint_device(size, axes, e, g, batch_shape=k)
+            system.field_adjoint_device(size, axes, e, g, centers_per_region=cb)
             torch.cuda.synchronize()
-            np.testing.assert_array_equal(e.cpu().numpy(), ref_e)
-            np.testing.assert_array_equal(g.cpu().numpy(), ref_g)
+            ref_e, ref_g = e.cpu().numpy(), g.cpu().numpy()
+            probe = VextBatch([system], size, axes,
+                              [torch.empty(shape, dtype=torch.float32, device="cuda")],
+                              gradients=[torch.empty(shape + (6,), dtype=torch.float32,
+                                                     device="cuda")],
+                              centers_per_region=cb)
+            n_adj = len({t["shape"] for t in probe.tuning()})
+            probe.close()
+            assert n_adj >= min_shapes
+            for k in range(1, n_adj + 1):
+                e = torch.empty(shape, dtype=torch.float32, device="cuda")
+                g = torch.empty(shape + (6,), dtype=torch.float32, device="cuda")
+                system.field_adjoint_device(size, axes, e, g, batch_shape=k,
+                                            centers_per_region=cb)
+                torch.cuda.synchronize()
+                np.testing.assert_array_equal(e.cpu().numpy(), ref_e)
+                np.testing.assert_array_equal(g.cpu().numpy(), ref_g)
         fwd_ref = None
         for k in range(1, 3):
             out = torch.empty(shape, dtype=torch.float32, device="cuda")
