@@ -434,6 +434,9 @@ static const BatchKernel kAdjointFlush64Kernels[] = {   // accuracy/speed study
     {batch_field_kernel<16, 8, 4, 2, 7>, 128, "128x4 flush64"}};
 // 8-center regions x 64-director items (the same 512 poses per staged
 // entry): a smaller region radius, hence shorter near and shell lists
+static const BatchKernel kForwardCb8Kernels[] = {
+    {batch_field_kernel<8, 16, 4, 4, 0>, 128, "8c 128x4"},
+    {batch_field_kernel<8, 32, 2, 3, 0>, 256, "8c 256x2"}};
 static const BatchKernel kAdjointCb8Kernels[] = {
     {batch_field_kernel<8, 16, 4, 3, 8>, 128, "8c 128x4/3 gsum"},
     {batch_field_kernel<8, 16, 4, 2, 1>, 128, "8c 128x4"}};
@@ -445,7 +448,7 @@ constexpr int kMaxCandidates = 12;
 // 2 with the reciprocal of q^3 and a Newton step, 3 the same without it,
 // 4 / 5 default with FP32 gradient partials over 16 / 64 entries (a whole
 // 128-entry chunk by default; the energy partials always cover 16), 6 default
-// on 8-center regions with 64-director items
+// on 8-center regions with 64-director items, 7 forward on 8-center regions
 static int batch_kernel_count(int kind) {
     switch (kind) {
     case 0: return VEXT_COUNT(kForwardKernels);
@@ -454,6 +457,7 @@ static int batch_kernel_count(int kind) {
     case 4: return VEXT_COUNT(kAdjointFlush16Kernels);
     case 5: return VEXT_COUNT(kAdjointFlush64Kernels);
     case 6: return VEXT_COUNT(kAdjointCb8Kernels);
+    case 7: return VEXT_COUNT(kForwardCb8Kernels);
     default: return VEXT_COUNT(kAdjointRcp3Kernels);
     }
 }
@@ -466,24 +470,28 @@ static const BatchKernel &batch_kernel(int kind, int shape) {
     case 4: return kAdjointFlush16Kernels[shape];
     case 5: return kAdjointFlush64Kernels[shape];
     case 6: return kAdjointCb8Kernels[shape];
+    case 7: return kForwardCb8Kernels[shape];
     default: return kAdjointRcp3Kernels[shape];
     }
 }
 
-// The kernel table of a batch: forward (0), the forward + adjoint studies
-// (2-5, selected by variant bits), forward + adjoint on 16-center regions
-// (1, centers_per_region 16 or 32) or, by default, on 8-center regions (6).
+// The kernel table of a batch: forward on 16-center regions (0,
+// centers_per_region 16 or 32) or, by default, on 8-center regions (7); the
+// forward + adjoint studies (2-5, selected by variant bits), forward +
+// adjoint on 16-center regions (1) or, by default, on 8-center regions (6).
 static int batch_kind(const Options &o, bool adj) {
-    if (!adj) return 0;
+    const bool cb16 = o.cb == 16 || o.cb == 32;
+    if (!adj) return cb16 ? 0 : 7;
     if (o.variant & 32) return 2;
     if (o.variant & 64) return 3;
     if (o.variant & 128) return 4;
     if (o.variant & 512) return 5;
-    return o.cb == 16 || o.cb == 32 ? 1 : 6;
+    return cb16 ? 1 : 6;
 }
 
 int batch_item_directors(const Options &o, bool adj) {
-    return batch_kind(o, adj) == 6 ? 64 : 32;
+    const int kind = batch_kind(o, adj);
+    return kind == 6 || kind == 7 ? 64 : 32;
 }
 
 }  // namespace vext
@@ -594,7 +602,7 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
     VEXT_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     VEXT_CUDA(cudaMalloc(&b->d_axes, sizeof(double) * 3 * n_axes));
     VEXT_CUDA(cudaMemcpy(b->d_axes, axes, sizeof(double) * 3 * n_axes, cudaMemcpyHostToDevice));
-    // regions of 16 centers x items of 32 directors, or 8 x 64 (kind 6)
+    // regions of 16 centers x items of 32 directors, or 8 x 64 (kinds 6, 7)
     const int kOB = batch_item_directors(b->opt, b->adj), cb = 512 / kOB;
     std::vector<BatchSys> hs(n_systems);
     std::vector<std::pair<long long, int4>> items;
