@@ -371,8 +371,9 @@ VEXT_API int vext_measure_pipes(int iterations, double *ffma_per_s, double *ffma
 
 /* Exact FP64 number of (site, image) pairs closer than the cutoff over the
  * size^3 x n_axes field (the algorithmic unit of work); far_pairs (may be
- * NULL) receives those whose image is a far entry for the given r_split
- * (<= 0: the default), i.e. the pairs the FP32 far kernel evaluates. */
+ * NULL) receives those whose image is a far entry of the default 16-center
+ * regions for the given r_split (<= 0: the default), i.e. the pairs the FP32
+ * far kernel of the mixed field evaluates. */
 VEXT_API int vext_count_pairs(vext_system sys, int size, int n_axes, const double *axes,
                               double r_split, int64_t *pairs, int64_t *far_pairs);
 

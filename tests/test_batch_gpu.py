@@ -1,9 +1,9 @@
 """Batched fields (one persistent, graph-captured launch over many systems)
-through the C ABI: on 16-center regions each system's output equals its own
-single-field mixed-precision result bit for bit (same lists, same pair loops,
-same order); on the default 8-center regions (other lists, so other rounding)
-it agrees with the FP64 kernel within the stated tolerance; replays
-reproduce both bit for bit."""
+through the C ABI: each system's output equals its own single-field
+mixed-precision result on the same region size bit for bit (same lists,
+same pair loops, same order) -- 8-center regions, the batch default, and 16,
+the single-field default -- agrees with the FP64 kernel within the stated
+tolerance, and replays reproduce it."""
 import numpy as np
 import pytest
 import torch
@@ -31,7 +31,7 @@ def test_batch_matches_single_fields():
         batch16.check()
         torch.cuda.synchronize()
         for case, system, out in zip(cases, systems, outs16):
-            single = system.field(size, axes)["orientation_K"]
+            single = system.field(size, axes)["orientation_K"]     # 16-center regions
             np.testing.assert_array_equal(out.cpu().numpy(), single)
     batch16.close()
     outs = [torch.full((64, size, size, size), -1.0, dtype=torch.float32, device="cuda")
@@ -51,6 +51,9 @@ def test_batch_matches_single_fields():
             first = got
         for a, b in zip(first, got):
             np.testing.assert_array_equal(a, b)
+        for system, out in zip(systems, got):
+            single = system.field(size, axes, centers_per_region=8)["orientation_K"]
+            np.testing.assert_array_equal(out, single)
     for case, system, out in zip(cases, systems, outs):
         exact = system.field(size, axes, mode=_lib.VEXT_MODE_FP64, energy=True,
                              orientation=False)["energy"].T.reshape(64, size, size, size)
