@@ -2,7 +2,9 @@
 // shapes) in ONE persistent launch over a work queue, captured in a CUDA
 // graph and replayed.
 //
-// Work item = (system, region, director block).  Items are sorted by
+// Work item = (system, region, director block): by default an 8-center
+// region x 64 directors (16 x 32 with centers_per_region 16; either way one
+// staged list entry serves 512 poses).  Items are sorted by
 // estimated cost (list length, longest first) so the tail of the queue is
 // made of short items; resident CTAs claim items with one atomicAdd each.
 // Each item runs the near (FP64) and the far (packed FP32x2) pair loops of
@@ -12,10 +14,11 @@
 // refinement band are appended to a list that batch_refine_kernel
 // recomputes in FP64.
 //
-// Autotuning: the CTA shape (128 threads x 4 directors or 256 threads x 2
-// directors, both covering a 32-director block) and the number of resident
-// CTAs per SM are chosen by timing each candidate on a strided 1/16 sample of
-// the queue at creation; the winner is captured into the graph.  The batch
+// Autotuning: the CTA shape of the mode's table (128 threads x 4 directors
+// or 256 threads x 2, register-resident or shared-memory gradient sums) and
+// the number of resident CTAs per SM are chosen by timing each candidate on
+// a strided 1/16 sample of the queue at creation; the winner is captured
+// into the graph.  The batch
 // keeps pointers to its systems' region lists: the systems must outlive it
 // and not be invalidated while it exists.
 #include <algorithm>
@@ -401,10 +404,12 @@ struct BatchConfig {
     int grid;    // resident CTAs (persistent grid)
 };
 
-// CTA shapes the autotuner chooses from; every shape covers a 32-director
-// block (G x P = 32).  Forward: <16, 8, 4> x 128 threads or <16, 16, 2> x 256.
-// Forward + adjoint (9 FP64 sums per director): <16, 16, 2> x 256, or
-// <16, 8, 4> x 128 bounded to 2 or 3 CTAs per SM (225 / 168 registers).
+// CTA shapes <CB centers, G director groups, P directors per thread> the
+// autotuner chooses from; a table's shapes share CB and the director block
+// G x P (16 x 32 or 8 x 64).  Forward: 128 threads x 4 directors or 256 x 2.
+// Forward + adjoint (9 FP64 sums per director): 256 x 2, or 128 x 4 bounded
+// to 2 or 3 CTAs per SM (225 / 168 registers), or 128 x 4 with the FP64
+// gradient sums in shared memory (162 registers, 3 CTAs per SM).
 struct BatchKernel {
     void (*fn)(BatchArgs);
     int threads;
