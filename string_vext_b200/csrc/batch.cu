@@ -444,7 +444,8 @@ static const BatchKernel kForwardCb8Kernels[] = {
     {batch_field_kernel<8, 32, 2, 3, 0>, 256, "8c 256x2"}};
 static const BatchKernel kAdjointCb8Kernels[] = {
     {batch_field_kernel<8, 16, 4, 3, 8>, 128, "8c 128x4/3 gsum"},
-    {batch_field_kernel<8, 16, 4, 2, 1>, 128, "8c 128x4"}};
+    {batch_field_kernel<8, 16, 4, 2, 1>, 128, "8c 128x4"},
+    {batch_field_kernel<8, 32, 2, 2, 1>, 256, "8c 256x2"}};
 constexpr int kMaxCandidates = 12;
 
 #define VEXT_COUNT(t) (int)(sizeof t / sizeof t[0])
