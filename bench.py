@@ -158,9 +158,12 @@ def cpu_reference_sample(case, size, n_axes, seconds_target, processes):
     energy, wall, used, compute = oracle.reference_field_parallel(
         case, sample, axes, library=library, processes=processes, symbol=symbol)
     poses = len(sample) * n_axes
+    which = ("reference driver (baseline/_ref)" if symbol == "evaluate_reused_neighbors"
+             and oracle.reference_driver_class() is not None else "restated driver (oracle)")
     return {"value": poses / compute, "unit": "poses/s", "cores": used, "kind": kind,
             "sample": f"{len(sample)} of {len(centers)} grid centers (stride {stride}) x "
-                      f"{n_axes} directors (forward energies only), {used} spawn processes; "
+                      f"{n_axes} directors (forward energies only), {used} spawn processes, "
+                      f"{which}; "
                       f"time = slowest worker's kd-tree query + kernel ({compute:.2f} s; "
                       f"{wall:.2f} s with process start), {cpu_model()}",
             "seconds": compute, "poses": poses}
@@ -179,7 +182,7 @@ def cpu_reference_single_core(case, size, n_axes, seconds_target):
     n_sample = int(min(len(centers), max(512, CPU_CENTERS_PER_CORE_S * seconds_target)))
     stride = max(1, len(centers) // n_sample)
     sample = centers[::stride][:n_sample]
-    driver = oracle.ReferenceDriver(case, library, symbol=symbol)
+    driver, which = oracle.cpu_driver(case, library, symbol)
     t0 = time.perf_counter()
     driver.evaluate(sample, axes)
     wall = time.perf_counter() - t0
@@ -188,7 +191,7 @@ def cpu_reference_single_core(case, size, n_axes, seconds_target):
             "kernel_only": poses / driver.compute_seconds,
             "query_share": driver.query_seconds / wall,
             "sample": f"{len(sample)} of {len(centers)} grid centers (stride {stride}) x "
-                      f"{n_axes} directors, one process; {wall:.2f} s, kd-tree query "
+                      f"{n_axes} directors, one process, {which}; {wall:.2f} s, kd-tree query "
                       f"{driver.query_seconds:.2f} s, kernel {driver.compute_seconds:.2f} s, "
                       f"{cpu_model()}"}
 
@@ -566,19 +569,34 @@ def bench_string_update():
                         "vext_string_run (graph-replayed iterations)"}
 
 
+def reference_package_driver():
+    """``NativeReusePotential`` of the reference package installed unchanged in
+    baseline/_ref (pip --target), or None when it is not installed."""
+    package = ROOT / "baseline" / "_ref"
+    if not (package / "string_vext" / "native.py").exists():
+        return None
+    if str(package) not in sys.path:
+        sys.path.append(str(package))
+    from string_vext.native import NativeReusePotential
+    return NativeReusePotential
+
+
 def bench_dropin(case, size, axes):
-    """The drop-in mode: the reference's own driver (restated in
-    string_vext_b200/native.py: host kd-tree query and CSR per 512-center
+    """The drop-in mode: the reference's own, unmodified driver (its package
+    installed in baseline/_ref: host kd-tree query and CSR per 512-center
     batch, one process) calling this library's evaluate_reused_neighbors, on
     the strided center sample of cpu_baseline_single_core.  Poses/s with the
     host query and for the library calls alone (host buffers in and out)."""
-    from string_vext_b200.native import NativeReusePotential
+    from string_vext_b200 import _lib
     from string_vext_b200.orientation import regular_pose_grid
+    driver_class = reference_package_driver()
+    if driver_class is None:
+        return {"unavailable": "reference package not installed in baseline/_ref"}
     centers, _ = regular_pose_grid(size, len(axes))
     n_sample = int(min(len(centers), max(512, CPU_CENTERS_PER_CORE_S * 5.0)))
     stride = max(1, len(centers) // n_sample)
     sample = centers[::stride][:n_sample]
-    pot = NativeReusePotential(case)
+    pot = driver_class(case, _lib.LIB_PATH)
     pot.evaluate(sample[:512], axes)          # device buffers and context
     pot.query_seconds = pot.compute_seconds = 0.0
     t0 = time.perf_counter()
@@ -591,7 +609,7 @@ def bench_dropin(case, size, axes):
             "sample": f"{len(sample)} of {len(centers)} grid centers (stride {stride}) x "
                       f"{len(axes)} directors, one process; {wall:.2f} s, kd-tree query "
                       f"{pot.query_seconds:.2f} s, library calls {pot.compute_seconds:.2f} s",
-            "path": "reference driver (kd-tree + CSR on the host) -> "
+            "path": "reference driver from baseline/_ref (kd-tree + CSR on the host) -> "
                     "evaluate_reused_neighbors of this library (FP64, bit-identical to the "
                     "reference kernel)"}
 

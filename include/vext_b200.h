@@ -60,20 +60,23 @@ VEXT_API int evaluate_reused_neighbors(int n_centers, int n_axes, int n_images, 
                               const double *shift, const double *floor2, const int64_t *starts,
                               const int32_t *indices, double *output);
 
-/* The same pair sum for callers that cannot allocate device memory: code
- * running inside CUDA stream capture (where cudaMalloc is not allowed),
- * plug-ins whose host runtime owns the GPU memory budget, real-time loops
- * that cannot afford an allocation's synchronisation.  It has no counterpart
- * in the reference.  Same arguments, host buffers, codes and bit-identical
- * output as evaluate_reused_neighbors, but it calls no cudaMalloc/cudaFree/
- * cudaMallocHost and uses no host heap: its scratch is one 64 MiB device
- * array compiled into the library (held by every GPU that loads it until
- * exit).  Batches needing more than 64 MiB of scratch (about 120 B per image +
- * 4 B per neighbour index + 8 B per output pose) return VEXT_ERR_CAPACITY.
- * The first call on each device resolves the array's address and loads its
- * module, so make it before any stream capture.  Calls are serialised inside
- * the process and finish before returning; the array keeps the last call's
- * contents, and overlapping calls would race on it. */
+/* The same pair sum for callers that cannot allocate device memory:
+ * plug-ins whose host runtime owns the GPU memory budget and allows no
+ * allocations of their own (fixed-pool servers, MPS clients with hard memory
+ * limits), real-time loops that cannot afford an allocation's implicit
+ * synchronisation.  It has no counterpart in the reference.  Same arguments,
+ * host buffers, codes and bit-identical output as evaluate_reused_neighbors,
+ * but it calls no cudaMalloc/cudaFree/cudaMallocHost and uses no host heap:
+ * its scratch is one 64 MiB device array compiled into the library (held by
+ * every GPU that loads it until exit).  Batches needing more than 64 MiB of
+ * scratch (about 120 B per image + 4 B per neighbour index + 8 B per output
+ * pose) return VEXT_ERR_CAPACITY before anything is copied to the device.
+ * The first call on each device loads the library's module there; every
+ * call looks the array's device address up with cudaGetSymbolAddress.  Work
+ * runs on the calling thread's per-thread default stream and is finished
+ * when the call returns; calls are serialised inside the process.  The array
+ * keeps the last call's contents, and calls that overlapped on the GPU would
+ * race on it. */
 VEXT_API int evaluate_reused_neighbors_noalloc(int n_centers, int n_axes, int n_images,
                                                double cutoff2, const double *centers,
                                                const double *axes, const double *images,
@@ -376,6 +379,15 @@ VEXT_API int vext_measure_pipes(int iterations, double *ffma_per_s, double *ffma
  * far kernel of the mixed field evaluates. */
 VEXT_API int vext_count_pairs(vext_system sys, int size, int n_axes, const double *axes,
                               double r_split, int64_t *pairs, int64_t *far_pairs);
+
+/* Exercises the device-wait timeout path: a kernel arms an mbarrier for a
+ * copy that is never issued and waits on it through the same bounded wait
+ * the staged pair kernels use, with `polls` (1 .. 2^22) as the limit.  Returns
+ * VEXT_ERR_TIMEOUT with a message when the wait gives up (the expected
+ * outcome); nothing is left in flight, so the device stays usable.  No
+ * reference counterpart: the reference kernels have no device waits
+ * (native/vext/kernel.cpp returns codes 1-4 only). */
+VEXT_API int vext_check_wait_timeout(int polls);
 
 /* Library version string. */
 VEXT_API const char *vext_version(void);

@@ -32,6 +32,8 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libvext_oracle.so"
 REF_KERNEL = HERE / "_ref" / "vext_kernel.so"
 REF_PAIR = HERE / "_ref" / "pair.so"
+#: The reference's Python package, installed unchanged (pip --target) beside the repo.
+REF_PACKAGE = HERE.parent / "baseline" / "_ref"
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _lib = None
@@ -261,10 +263,32 @@ class ReferenceDriver:
         return out
 
 
+def reference_driver_class():
+    """The reference's own ``NativeReusePotential`` (src/string_vext/native.py)
+    when its package is installed in ``baseline/_ref``, else None."""
+    if not (REF_PACKAGE / "string_vext" / "native.py").exists():
+        return None
+    import sys
+    if str(REF_PACKAGE) not in sys.path:
+        sys.path.append(str(REF_PACKAGE))
+    from string_vext.native import NativeReusePotential
+    return NativeReusePotential
+
+
+def cpu_driver(case, library, symbol="evaluate_reused_neighbors"):
+    """The reference CPU path's driver: the reference's own class when its
+    package is installed and the symbol is the reference's, else the
+    restatement above.  Returns (driver, which)."""
+    cls = reference_driver_class() if symbol == "evaluate_reused_neighbors" else None
+    if cls is not None:
+        return cls(case, library), "reference driver (baseline/_ref)"
+    return ReferenceDriver(case, library, symbol=symbol), "restated driver (oracle)"
+
+
 def _shard_worker(args):
     case, library, centers, axes, symbol = args
     os.environ.setdefault("OMP_NUM_THREADS", "1")
-    driver = ReferenceDriver(case, library, symbol=symbol)
+    driver, _ = cpu_driver(case, library, symbol)
     t0 = time.perf_counter()
     out = driver.evaluate(centers, axes)
     return out, time.perf_counter() - t0, driver.query_seconds, driver.compute_seconds

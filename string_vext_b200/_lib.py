@@ -21,6 +21,10 @@ VEXT_MODE_FP64 = 1
 VEXT_MODE_FP64_PLAIN = 2
 VEXT_MODE_FP32_NAIVE = 3
 
+VEXT_ERR_TIMEOUT = 17
+VEXT_ERR_ARGUMENT = 18
+VEXT_ERR_CAPACITY = 19
+
 STATUS = {0: "ok", 1: "bad sizes", 2: "CSR starts decreasing", 3: "CSR index out of range",
           4: "non-finite energy", 16: "CUDA error", 17: "device wait timeout",
           18: "invalid argument", 19: "capacity exceeded", 20: "out of memory"}
@@ -80,9 +84,15 @@ class VextError(RuntimeError):
 _lib = None
 
 
-def load() -> ctypes.CDLL:
-    """Load the library once; raise if it is missing (no fallback)."""
-    global _lib
+def load(path=None) -> ctypes.CDLL:
+    """Load the library once; raise if it is missing (no fallback).  ``path``
+    selects another build of the library; it must be given before the first
+    load of the process."""
+    global _lib, LIB_PATH
+    if path is not None and Path(path).resolve() != LIB_PATH.resolve():
+        if _lib is not None:
+            raise RuntimeError(f"vext_b200 library already loaded from {LIB_PATH}")
+        LIB_PATH = Path(path)
     if _lib is not None:
         return _lib
     if not LIB_PATH.exists():
@@ -96,6 +106,8 @@ def load() -> ctypes.CDLL:
     lib.evaluate_reused_neighbors_noalloc.restype = ci
     lib.vext_last_error.argtypes = []
     lib.vext_last_error.restype = ctypes.c_char_p
+    lib.vext_check_wait_timeout.argtypes = [ci]
+    lib.vext_check_wait_timeout.restype = ci
     lib.vext_version.argtypes = []
     lib.vext_version.restype = ctypes.c_char_p
     lib.vext_default_options.argtypes = [ctypes.POINTER(Options)]

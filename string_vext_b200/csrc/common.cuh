@@ -74,12 +74,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return done != 0;
 }
 
+__device__ __forceinline__ void mbar_inval(uint64_t *bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 // Bounded wait on one phase of an mbarrier.  Returns false (and records
-// DEV_TIMEOUT) if the phase did not complete within kWaitLimit polls.
+// DEV_TIMEOUT) if the phase did not complete within `limit` polls.
 // Once any CTA has recorded a failure, other waits give up at their next
 // status poll instead of spinning to their own limit.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *status) {
-    for (uint32_t it = 0; it < kWaitLimit; ++it) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *status,
+                                                  uint32_t limit = kWaitLimit) {
+    for (uint32_t it = 0; it < limit; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
         if ((it & 1023u) == 1023u && *(volatile int *)status != DEV_OK) return false;
     }

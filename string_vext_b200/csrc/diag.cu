@@ -60,9 +60,48 @@ __global__ void __launch_bounds__(256) rcp_peak_kernel(int iterations, float see
     if (s != s) sink[threadIdx.x] = s;
 }
 
+// A staged wait that can never complete: one thread arms the barrier for a
+// 16-byte copy that is never issued, then every thread waits through
+// mbar_wait_bounded with `polls` as its limit -- the path each staged pair
+// kernel takes when a copy does not land.  Nothing is in flight, so the
+// barrier is simply invalidated before the CTA exits.
+__global__ void wait_timeout_kernel(uint32_t polls, int *status) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(&bar, 16);
+    __syncthreads();
+    mbar_wait_bounded(&bar, 0, status, polls);
+    __syncthreads();
+    if (threadIdx.x == 0) mbar_inval(&bar);
+}
+
 }  // namespace vext
 
 using namespace vext;
+
+extern "C" int vext_check_wait_timeout(int polls) {
+    if (polls < 1 || (uint32_t)polls > kWaitLimit)
+        return fail(VEXT_ERR_ARGUMENT, "polls must lie in [1, %u]", kWaitLimit);
+    int *status = nullptr;
+    VEXT_CUDA(cudaMalloc(&status, sizeof(int)));
+    int h = DEV_OK;
+    cudaError_t err = cudaMemset(status, 0, sizeof(int));
+    if (err == cudaSuccess) {
+        wait_timeout_kernel<<<1, 32>>>((uint32_t)polls, status);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) err = cudaMemcpy(&h, status, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(status);
+    if (err != cudaSuccess)
+        return fail(VEXT_ERR_CUDA, "wait_timeout_kernel: %s", cudaGetErrorString(err));
+    if (h == DEV_TIMEOUT)
+        return fail(VEXT_ERR_TIMEOUT, "a bounded device wait gave up after %d polls", polls);
+    return h == DEV_OK ? 0 : fail(VEXT_ERR_CUDA, "unexpected device status %d", h);
+}
 
 // ops/s of one probe kernel (kind 0: FFMA, 1: FFMA2 counted as 2 FMAs, 2: RCP)
 static int probe(int kind, int iterations, double *ops) {

@@ -1,11 +1,11 @@
 // evaluate_reused_neighbors_noalloc: the drop-in CSR pair sum for callers
 // that must not allocate device memory.
 //
-// Who needs this: code that runs while a CUDA stream is being captured into a
-// graph (cudaMalloc is not allowed during capture), plug-ins hosted by a
-// runtime that owns the GPU memory budget and forbids allocations of its own
-// (fixed-pool inference servers, MPS clients with hard memory limits), and
-// real-time loops where an allocation's implicit synchronisation is
+// Who needs this: plug-ins hosted by a runtime that owns the GPU memory
+// budget and forbids allocations of its own (fixed-pool inference or
+// simulation servers, MPS clients with hard memory limits, applications that
+// hand out device memory only through their own allocator), and real-time
+// loops where an allocation's implicit device synchronisation is
 // unacceptable.  The regular entry point grows cached device buffers with
 // cudaMalloc on demand; this one never calls cudaMalloc, cudaFree,
 // cudaMallocHost or any allocating library routine, and uses no host heap.
@@ -17,24 +17,30 @@
 //   + 8 n_centers n_axes   (+ 256-byte alignment per part)  <=  64 MiB,
 // e.g. 165,000 images, 512 centers x 64 directors and 800,000 neighbours
 // take about 23 MiB.
-// Larger batches are rejected with VEXT_ERR_CAPACITY before anything is read
-// or copied.
+// Larger batches are rejected with VEXT_ERR_CAPACITY before anything is
+// copied to the device (the host checks of codes 2 and 3 come first and read
+// starts and indices).
 //
-// In host code `g_noalloc_scratch` only names a host-side stand-in; the device
-// address comes from cudaGetSymbolAddress, called once per device with that
-// device current, on the first call made on that device.  That first call also
-// loads the module holding the array, so it must happen before any stream
-// capture begins.  Every call reuses the same array and leaves the previous
-// call's contents in it; nothing in it has to start at zero (each call writes
-// every byte it reads).  Calls are serialised by a process-wide mutex and
-// complete before returning, so calls from this process never overlap on the
-// GPU; concurrent use of the array by overlapping calls would race.
+// In host code `g_noalloc_scratch` only names a host-side stand-in; the
+// device address comes from cudaGetSymbolAddress with the calling thread's
+// current device, checked and passed to the kernels.  The first call on a
+// device also loads the module holding the array there.  The address is
+// looked up again on every call (a lookup, not an allocation), so a device
+// reset between calls cannot leave a stale address behind.  Every call
+// reuses the same array and leaves the previous call's contents in it;
+// nothing in it has to start at zero (each call writes every byte it reads
+// before reading it; the one word that must start from a known value, the
+// first non-finite index, is set by a copy each call).  Calls are serialised
+// by a process-wide mutex and complete before returning, so calls from this
+// process never overlap on the GPU; calls that did overlap on the GPU (from
+// another process sharing the module, or by bypassing the mutex) would race
+// on the array.
 //
 // Semantics are those of evaluate_reused_neighbors (same arguments, host
 // buffers, return codes 0-4 in the reference's order, bit-identical FP64
 // output, only the prefix the reference writes on code 4), plus
 // VEXT_ERR_CAPACITY.  Work is issued on the calling thread's per-thread
-// default stream.
+// default stream, and the call returns when it is done.
 #include <cmath>
 #include <mutex>
 
@@ -48,24 +54,16 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 namespace {
 
-constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_lock;
-unsigned char *g_noalloc_ptr[kMaxDevices] = {};
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Device address of the scratch array on the current device (set-up on the
-// first call per device).
+// Device address of the scratch array on the current device.
 int scratch_address(unsigned char **out) {
-    int dev = 0;
-    VEXT_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return fail(VEXT_ERR_ARGUMENT, "device %d out of range", dev);
-    if (!g_noalloc_ptr[dev]) {
-        void *p = nullptr;
-        VEXT_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        g_noalloc_ptr[dev] = static_cast<unsigned char *>(p);
-    }
-    *out = g_noalloc_ptr[dev];
+    void *p = nullptr;
+    VEXT_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    if (!p) return fail(VEXT_ERR_CUDA, "no device address for the no-alloc scratch array");
+    *out = static_cast<unsigned char *>(p);
     return 0;
 }
 

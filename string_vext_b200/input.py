@@ -1,10 +1,20 @@
-"""Native String ``input.dat`` reader for neutral two-site guests.
+"""The native String ``input.dat`` layout, for neutral two-site guests.
 
-Mirrors the reference ``parse_string_input`` (src/string_vext/input.py:11-57):
-the same section headers are located, the same validity rules apply (two
-neutral sites, neutral numbered framework atoms, positive LJ parameters,
-site masses summing to the declared total) and the same case dictionary is
-returned, so a case parsed here can be handed to either implementation.
+The file is a sequence of labelled blocks: a label line (``La Lb Lc dL``,
+``Alpha Beta Gamma``, ``cutoff(A) ...``, ``Number of sites``, ``Number of
+atoms`` ...) followed by its value lines.  A site block is a count line, a
+column header, then one ``x y z epsilon sigma charge mass`` row per site; a
+framework block is a count line, a column header, then one ``id sigma
+epsilon charge mass frac_a frac_b frac_c [name]`` row per atom (the layout the
+reference String program reads, native/string/source_code/RC_main.cu:282-390).
+
+``parse_string_input`` returns the reference's case dictionary and enforces
+its acceptance rules with its messages (src/string_vext/input.py:11-57): two
+neutral sites with positive LJ parameters and masses summing to the declared
+total, neutral framework atoms numbered 1..N with positive sigma and
+epsilon, a positive cutoff and temperature.  The guest is stored canonically:
+both sites on the body x axis at their signed distance from the centre of
+mass, which fixes the site offsets the energy kernels use.
 """
 from __future__ import annotations
 
@@ -14,56 +24,82 @@ import numpy as np
 
 from .cell import cell_matrix
 
+#: Label prefixes of the blocks the parser reads.
+LENGTHS, ANGLES, CONDITIONS = "La Lb Lc", "Alpha Beta Gamma", "cutoff(A)"
+SITES, ATOMS = "Number of sites", "Number of atoms"
 
-def _row_after(lines, prefix):
-    for number, line in enumerate(lines):
-        if line.startswith(prefix):
-            return number + 1
-    raise ValueError(f"input section {prefix!r} missing")
+_REJECT = "invalid or charged two-site String input"
+
+
+class _Blocks:
+    """Value lines of an input file addressed by the label that precedes them."""
+
+    def __init__(self, text: str):
+        self.lines = [line.strip() for line in text.splitlines()]
+        self.start = {}
+        for number, line in enumerate(self.lines):
+            for label in (LENGTHS, ANGLES, CONDITIONS, SITES, ATOMS):
+                if line.startswith(label) and label not in self.start:
+                    self.start[label] = number + 1
+
+    def first(self, label: str) -> int:
+        if label not in self.start:
+            raise ValueError(f"input section {label!r} missing")
+        return self.start[label]
+
+    def numbers(self, row: int, width: int | None = None) -> list[float]:
+        fields = self.lines[row].split() if row < len(self.lines) else []
+        return [float(v) for v in (fields if width is None else fields[:width])]
+
+    def table(self, label: str, width: int) -> np.ndarray:
+        """The counted table of a block: count line, header line, rows."""
+        at = self.first(label)
+        count = int(self.lines[at])
+        if count < 0:
+            raise ValueError(_REJECT)
+        rows = [self.numbers(at + 2 + k, width) for k in range(count)]
+        if any(len(r) != width for r in rows):
+            raise ValueError(_REJECT)
+        return np.array(rows, dtype=float).reshape(count, width)
+
+
+def _accept(guest: np.ndarray, frame: np.ndarray, conditions: list[float]) -> bool:
+    numbered = np.array_equal(frame[:, 0], np.arange(1, len(frame) + 1))
+    return (guest.shape == (2, 7) and len(frame) >= 1 and len(conditions) >= 4 and numbered
+            and all(np.isfinite(a).all() for a in (guest, frame, np.array(conditions)))
+            and not guest[:, 5].any() and not frame[:, 3].any()
+            and (guest[:, 3:5] > 0).all() and (guest[:, 6] > 0).all()
+            and (frame[:, 1:3] > 0).all() and conditions[0] > 0 and conditions[3] > 0)
 
 
 def parse_string_input(path) -> dict:
-    lines = [line.strip() for line in Path(path).read_text().splitlines()]
-    lengths = [float(v) for v in lines[_row_after(lines, "La Lb Lc")].split()[:3]]
-    angles = [float(v) for v in lines[_row_after(lines, "Alpha Beta Gamma")].split()[:3]]
+    blocks = _Blocks(Path(path).read_text())
+    lengths = blocks.numbers(blocks.first(LENGTHS), 3)
+    angles = blocks.numbers(blocks.first(ANGLES), 3)
     cell = cell_matrix(lengths, angles)
-    conditions = [float(v) for v in lines[_row_after(lines, "cutoff(A)")].split()]
-    g0 = _row_after(lines, "Number of sites")
-    n_guest = int(lines[g0])
-    guest = np.array([[float(v) for v in row.split()[:7]]
-                      for row in lines[g0 + 2:g0 + 2 + n_guest]])
-    f0 = _row_after(lines, "Number of atoms")
-    n_frame = int(lines[f0])
-    frame = np.array([[float(v) for v in row.split()[:8]]
-                      for row in lines[f0 + 2:f0 + 2 + n_frame]])
-    if (guest.shape != (2, 7) or frame.shape != (n_frame, 8)
-            or len(conditions) < 4 or not np.isfinite(guest).all()
-            or not np.isfinite(frame).all() or not np.isfinite(conditions).all()
-            or not np.array_equal(frame[:, 0], np.arange(1, n_frame + 1))
-            or (guest[:, 5] != 0).any() or (frame[:, 3] != 0).any()
-            or (guest[:, 3:5] <= 0).any() or (guest[:, 6] <= 0).any()
-            or (frame[:, 1:3] <= 0).any() or conditions[0] <= 0
-            or conditions[3] <= 0):
-        raise ValueError("invalid or charged two-site String input")
+    conditions = blocks.numbers(blocks.first(CONDITIONS))   # rc, FH flag, mass, T, steps
+    guest = blocks.table(SITES, 7)
+    frame = blocks.table(ATOMS, 8)
+    if not _accept(guest, frame, conditions):
+        raise ValueError(_REJECT)
+    cutoff, total, temperature = conditions[0], conditions[2], conditions[3]
     mass = guest[:, 6]
-    total = conditions[2]
     if not np.isclose(mass.sum(), total, rtol=1e-7):
         raise ValueError("guest site masses differ from declared total mass")
-    body = guest[:, :3]
-    separation = body[1] - body[0]
-    bond = np.linalg.norm(separation)
+    xyz = guest[:, :3]
+    axis = xyz[1] - xyz[0]
+    bond = np.linalg.norm(axis)
     if bond <= 0:
         raise ValueError("two distinct guest sites required")
-    director = separation / bond
-    com = (body * mass[:, None]).sum(0) / total
-    canonical = np.zeros((2, 3))
-    canonical[:, 0] = (body - com) @ director
+    centre = (xyz * mass[:, None]).sum(0) / total
+    body = np.zeros((2, 3))
+    body[:, 0] = (xyz - centre) @ (axis / bond)
     return {"cell": cell, "frame_frac": np.mod(frame[:, 5:8], 1),
             "frame_sigma": frame[:, 1], "frame_epsilon": frame[:, 2],
-            "guest_xyz": canonical, "guest_sigma": guest[:, 4],
+            "guest_xyz": body, "guest_sigma": guest[:, 4],
             "guest_epsilon": guest[:, 3], "guest_mass": mass,
-            "total_mass": float(total), "temperature": float(conditions[3]),
-            "cutoff": float(conditions[0]), "cell_lengths": lengths,
+            "total_mass": float(total), "temperature": float(temperature),
+            "cutoff": float(cutoff), "cell_lengths": lengths,
             "cell_angles_deg": angles, "bond_length": float(bond)}
 
 
@@ -72,7 +108,7 @@ def write_string_input(case: dict, path, n_points: int = 401, delta_frac: float 
                        running_steps: int = 10000) -> None:
     """Write a case in the native ``input.dat`` layout (the inverse of
     ``parse_string_input``), e.g. for handing a synthetic framework to the
-    reference CLI or to the String driver."""
+    reference String program or its Python CLI."""
     lengths = case["cell_lengths"]
     angles = case["cell_angles_deg"]
     frac = np.asarray(case["frame_frac"], dtype=float)

