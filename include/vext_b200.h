@@ -149,7 +149,10 @@ typedef struct {
     int variant;             /* pair-kernel shape; 0 = default                */
     int batch_shape;         /* batches: 1 + index of the CTA shape to run at
                                 full occupancy instead of autotuning; 0 =
-                                autotune (vext_batch_tuning lists the shapes) */
+                                autotune (vext_batch_tuning lists the shapes);
+                                the autotuner keeps its pick per size class
+                                for the process, and variant bit 2048 makes a
+                                batch time its candidates afresh             */
     int reserved[2];
 } vext_options;
 
@@ -248,7 +251,8 @@ VEXT_API int vext_pose_energy_grad_device(vext_system sys, int n, const double *
  * the positions, energy check of the new angles, angle smoothing, movement-
  * based convergence test every check_every iterations -- the same rules and
  * constants -- with the finite-difference forces replaced by h x the analytic
- * gradient.  path is HOST [n][6] (fractional a, b, c; Euler alpha, beta,
+ * gradient (or, with params->gradient = VEXT_STRING_REFERENCE_FD, the
+ * reference's own differences, which reproduce its path files).  path is HOST [n][6] (fractional a, b, c; Euler alpha, beta,
  * gamma in radians, R = Rz(gamma) Ry(beta) Rx(alpha)), updated in place;
  * energy (may be NULL) receives the final energies [n]. */
 typedef struct {
@@ -261,7 +265,14 @@ typedef struct {
     double conv_rot_percent;
     int max_iterations;        /* Running_steps                                 */
     int check_every;           /* convergence test period (200)                 */
+    int gradient;              /* VEXT_STRING_ANALYTIC (default): h x the
+                                  analytic gradient; VEXT_STRING_REFERENCE_FD:
+                                  the reference's own one-sided differences
+                                  E(x + h e_k) - E(x) (global.h:1141-1325),
+                                  seven pose energies per image per iteration */
 } vext_string_params;
+
+enum { VEXT_STRING_ANALYTIC = 0, VEXT_STRING_REFERENCE_FD = 1 };
 
 typedef struct {
     int iterations;            /* iterations run (the reference's i_time)       */

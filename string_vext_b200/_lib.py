@@ -60,7 +60,11 @@ class StringParams(ctypes.Structure):
                 ("delta_angle_rad", ctypes.c_double), ("smooth", ctypes.c_double),
                 ("rounding", ctypes.c_double), ("conv_trans_percent", ctypes.c_double),
                 ("conv_rot_percent", ctypes.c_double), ("max_iterations", ctypes.c_int),
-                ("check_every", ctypes.c_int)]
+                ("check_every", ctypes.c_int), ("gradient", ctypes.c_int)]
+
+
+VEXT_STRING_ANALYTIC = 0
+VEXT_STRING_REFERENCE_FD = 1
 
 
 class StringResult(ctypes.Structure):

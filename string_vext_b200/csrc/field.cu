@@ -525,39 +525,10 @@ __global__ void __launch_bounds__(256)
         frac_to_cart(a.H, (gi + .5) / a.S - r.of[0], (gj + .5) / a.S - r.of[1],
                      (gk + .5) / a.S - r.of[2], cx, cy, cz);
         const double u[3] = {a.axes[3 * o], a.axes[3 * o + 1], a.axes[3 * o + 2]};
-        double e = 0.0, gc[3] = {0, 0, 0}, gu[3] = {0, 0, 0};
-        for (int s = 0; s < 2; ++s) {
-            const double off = s ? a.off1 : a.off0;
-            const double px = cx + off * u[0], py = cy + off * u[1], pz = cz + off * u[2];
-            double gs[3] = {0, 0, 0};
-            for (int k = 0; k < r.n_total; ++k) {
-                const float4 h = a.hi[r.off + k], l = a.lo[r.off + k];
-                const double dx = px - ((double)h.x + (double)l.x);
-                const double dy = py - ((double)h.y + (double)l.y);
-                const double dz = pz - ((double)h.z + (double)l.z);
-                const double d2 = dx * dx + dy * dy + dz * dz;
-                if (d2 >= a.rc2) continue;
-                const int t = __float_as_int(h.w);
-                const double c12 = a.td[4 * t], c6 = a.td[4 * t + 1], fl = a.td[4 * t + 3];
-                const double s2 = d2 < fl ? fl : d2;
-                const double i2 = 1.0 / s2;
-                const double i6 = i2 * i2 * i2;
-                e += c12 * i6 * i6 - c6 * i6 + a.td[4 * t + 2];
-                if (d2 >= fl) {
-                    const double de = 2.0 * (-6.0 * c12 * i6 * i6 + 3.0 * c6 * i6) * i2;
-                    gs[0] += de * dx;
-                    gs[1] += de * dy;
-                    gs[2] += de * dz;
-                }
-            }
-            for (int k = 0; k < 3; ++k) {
-                gc[k] += gs[k];
-                gu[k] += off * gs[k];
-            }
-        }
-        const double uu = gu[0] * u[0] + gu[1] * u[1] + gu[2] * u[2];
-        const double g[6] = {gc[0], gc[1], gc[2], gu[0] - uu * u[0], gu[1] - uu * u[1],
-                             gu[2] - uu * u[2]};
+        double e = 0.0, g[6];
+        fp64_pose_pairs(a.hi, a.lo, a.td, r.off, r.n_total, 0, 1, a.rc2, a.off0, a.off1, cx, cy,
+                        cz, u, e, g);
+        fp64_tangent(u, g);
         if (e64) e64[idx] = e;
         if (e32) e32[idx] = (float)e;
         for (int k = 0; k < 6; ++k) {

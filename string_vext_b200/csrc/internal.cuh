@@ -78,6 +78,12 @@ struct System {
     int n_atoms = 0, n_types = 0;
     double guest_sigma = 0, guest_epsilon = 0, offsets[2] = {0, 0}, cutoff = 0, temperature = 0;
     double max_offset = 0;
+    // FNV-1a hash of the framework as the region lists see it (cell, cutoff,
+    // wrapped fractional coordinates, type ids and the framework (sigma,
+    // epsilon) of every type): systems with equal hashes differ only in the
+    // guest, so one region-list set serves them all when it is built for the
+    // largest site offset among them
+    uint64_t frame_hash = 0;
     double *d_frac = nullptr;
     int *d_type = nullptr;
     float4 *d_tf = nullptr;

@@ -174,6 +174,69 @@ __device__ __forceinline__ void near_chunk(const double *ed, const double *std4,
     }
 }
 
+// ------------------------------------------------------------ FP64 pose
+
+// FP64 energy and site-force sums of one pose over entries k = first,
+// first + step, ... of a region list (positions hi + lo relative to the
+// region origin; c the grid center there, u the director):
+//   e += sum over sites and in-cutoff pairs of c12 i6^2 - c6 i6 + shift,
+//   g[0..2] += dE/dc, g[3..5] += dE/du (not yet projected),
+// with d2 >= rc^2 out (the reference's test, kernel.cpp:29-30), the contact
+// floor on d2 and no force below it.  The same code serves the plain FP64
+// kernels (one thread per pose) and the FP64 re-evaluation of flagged poses
+// (a warp per pose), so both classify every pair identically.
+__device__ __forceinline__ void fp64_pose_pairs(const float4 *hi, const float4 *lo,
+                                                const double *td, long long off, int n,
+                                                int first, int step, double rc2, double off0,
+                                                double off1, double cx, double cy, double cz,
+                                                const double (&u)[3], double &e,
+                                                double (&g)[6]) {
+    for (int k = 0; k < 6; ++k) g[k] = 0.0;
+    for (int s = 0; s < 2; ++s) {
+        const double o = s ? off1 : off0;
+        const double px = cx + o * u[0], py = cy + o * u[1], pz = cz + o * u[2];
+        double gs[3] = {0, 0, 0};
+        for (int k = first; k < n; k += step) {
+            const float4 h = hi[off + k], l = lo[off + k];
+            const double dx = px - ((double)h.x + (double)l.x);
+            const double dy = py - ((double)h.y + (double)l.y);
+            const double dz = pz - ((double)h.z + (double)l.z);
+            const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
+            if (d2 >= rc2) continue;
+            const int t = __float_as_int(h.w);
+            const double c12 = td[4 * t], c6 = td[4 * t + 1], fl = td[4 * t + 3];
+            const double s2 = d2 < fl ? fl : d2;
+            const double i2 = 1.0 / s2;
+            const double i6 = i2 * i2 * i2;
+            e += c12 * i6 * i6 - c6 * i6 + td[4 * t + 2];
+            if (d2 >= fl) {
+                const double de = 2.0 * (-6.0 * c12 * i6 * i6 + 3.0 * c6 * i6) * i2;
+                gs[0] += de * dx;
+                gs[1] += de * dy;
+                gs[2] += de * dz;
+            }
+        }
+        for (int k = 0; k < 3; ++k) {
+            g[k] += gs[k];
+            g[3 + k] += o * gs[k];
+        }
+    }
+}
+
+// Project dE/du (g[3..5]) on the plane normal to the unit director u.
+__device__ __forceinline__ void fp64_tangent(const double (&u)[3], double (&g)[6]) {
+    const double uu = g[3] * u[0] + g[4] * u[1] + g[5] * u[2];
+    for (int k = 0; k < 3; ++k) g[3 + k] -= uu * u[k];
+}
+
+// A shell pair whose FP32 q lies within kBorderTol (A^2) of rc^2 may be
+// classified differently by the FP32 test than by the FP64 one.  The FP32 q
+// of a far entry carries at most about 6e-5 A^2 of error at r ~ 13 A (the
+// entry position rounded to FP32 relative to its region origin, 2 |d| x
+// 8.3e-7 A, plus the roundings of |d0|^2, t and the site FMA), so poses with
+// such a pair are re-evaluated in FP64.
+constexpr float kBorderTol = 1e-4f;
+
 // ------------------------------------------------------------ far (FP32x2)
 
 struct FarGeom {
@@ -181,6 +244,9 @@ struct FarGeom {
     float2 m0, m1;             // -2 o_s, broadcast
     float oo0, oo1;            // o_s^2
     float rc2f;
+    float2 mcx, mcy, mcz;      // -c, broadcast (expanded entries)
+    float2 oo02, oo12;         // o_s^2, broadcast (expanded entries)
+    float out2;                // |d0|^2 beyond which no site of the pose reaches rc
 };
 
 __device__ __forceinline__ FarGeom far_geom(double cxd, double cyd, double czd, double off0,
@@ -194,7 +260,42 @@ __device__ __forceinline__ FarGeom far_geom(double cxd, double cyd, double czd, 
     g.oo0 = (float)(off0 * off0);
     g.oo1 = (float)(off1 * off1);
     g.rc2f = rc2f;
+    g.mcx = make_float2(-g.cx, -g.cx);
+    g.mcy = make_float2(-g.cy, -g.cy);
+    g.mcz = make_float2(-g.cz, -g.cz);
+    g.oo02 = make_float2(g.oo0, g.oo0);
+    g.oo12 = make_float2(g.oo1, g.oo1);
+    // (rc + max|o| + 1e-3 A)^2: a site is at least |d0| - max|o| from the
+    // entry, so beyond this every pair is out by far more than FP32 rounding
+    const double rmax = sqrt((double)rc2f) + fmax(fabs(off0), fabs(off1)) + 1e-3;
+    g.out2 = (float)(rmax * rmax);
     return g;
+}
+
+// Expanded far entries: the packed FP32x2 loops take each scalar of an entry
+// as a (v, v) pair, so a staged chunk of (x, y, z, type) entries is rewritten
+// once per CTA as two float4 (x, x, y, y), (z, z, type, 0) that load straight
+// into register pairs; the pair coefficients of every type wait pre-paired in
+// the same way (far_types_x2).  The arithmetic and its rounding are those of
+// the scalar entries.
+template <int NT>
+__device__ __forceinline__ void far_expand(const float4 *hb, float4 *xb, int len) {
+    for (int e = threadIdx.x; e < len; e += NT) {
+        const float4 h = hb[e];
+        xb[2 * e] = make_float4(h.x, h.x, h.y, h.y);
+        xb[2 * e + 1] = make_float4(h.z, h.z, h.w, 0.f);
+    }
+}
+
+// Per type: (c12, c12, -c6, -c6), (-2 c12, -2 c12, c6, c6), (shift, shift, shift, 0).
+template <int NT>
+__device__ __forceinline__ void far_types_x2(float4 *stx, const float4 *tf, int n_types) {
+    for (int t = threadIdx.x; t < n_types; t += NT) {
+        const float4 p = tf[t];
+        stx[3 * t] = make_float4(p.x, p.x, -p.y, -p.y);
+        stx[3 * t + 1] = make_float4(-2.f * p.x, -2.f * p.x, p.y, p.y);
+        stx[3 * t + 2] = make_float4(p.z, p.z, p.z, 0.f);
+    }
 }
 
 // The earlier forward far chunk, kept for comparison with far_chunk_fwd:
@@ -459,15 +560,24 @@ __device__ __forceinline__ void grad_load(double *gsum, AdjAcc (&acc)[P]) {
 // the energy every 16 entries, the gradient sums every FLUSH entries.
 // GSUM_NT > 0: the gradient partials go to the shared-memory sums
 // (grad_slot<GSUM_NT>(gsum, ...)) instead of acc (whose energies stay).
+// border (masked entries only, when non-null): per director the smallest
+// |q - rc^2| met, so that poses with a pair whose FP32 q lies too close to
+// the cutoff for the FP32 test to decide it like the FP64 one can be
+// re-evaluated in FP64 (the force jumps at rc, so a pair counted on the
+// other side moves the gradient by the jump).
+// X2: hb holds expanded entries (far_expand) and stf the pre-paired type
+// table (far_types_x2); same results, fewer instructions per entry.
 template <int P, bool NEWTON, int FLUSH, bool MASK, bool RCP1 = true, int UNROLL = 1,
-          int GSUM_NT = 0>
+          int GSUM_NT = 0, bool BORDER = false, bool X2 = false>
 __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *stf, int len,
                                               const FarGeom &g, const float2 (&ux)[P / 2],
                                               const float2 (&uy)[P / 2],
                                               const float2 (&uz)[P / 2], AdjAcc (&acc)[P],
-                                              double &shift_sum, double *gsum = nullptr) {
+                                              double &shift_sum, double *gsum = nullptr,
+                                              float *border = nullptr) {
     constexpr int PP = P / 2;
     const float2 one2 = make_float2(1.f, 1.f);
+    const float2 mrc2 = make_float2(-g.rc2f, -g.rc2f);
 #pragma unroll 1
     for (int e0 = 0; e0 < len; e0 += FLUSH) {
         float2 fh[PP][2][3], ff[PP][2];
@@ -489,17 +599,50 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
         const int b1 = min(b0 + 16, e1);
 #pragma unroll UNROLL
         for (int e = b0; e < b1; ++e) {
-            const float4 h = hb[e];
-            const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, -)
-            const float dx = h.x - g.cx, dy = h.y - g.cy, dz = h.z - g.cz;
-            const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            const float2 k0 = make_float2(dd + g.oo0, dd + g.oo0),
-                         k1 = make_float2(dd + g.oo1, dd + g.oo1);
-            const float2 dx2 = make_float2(dx, dx), dy2 = make_float2(dy, dy),
-                         dz2 = make_float2(dz, dz);
-            const float2 c12 = make_float2(tp.x, tp.x), c6 = make_float2(tp.y, tp.y),
-                         sh = make_float2(tp.z, tp.z);
-            if (!MASK) fs += tp.z;
+            float2 k0, k1, dx2, dy2, dz2, c12, c6, sh, mc6, m2c12;
+            float4 tp;
+            if constexpr (X2) {
+                const float4 A = hb[2 * e], B = hb[2 * e + 1];
+                const float4 *tq = stf + 3 * __float_as_int(B.z);
+                const float4 T0 = tq[0], T1 = tq[1];
+                dx2 = __fadd2_rn(make_float2(A.x, A.y), g.mcx);
+                dy2 = __fadd2_rn(make_float2(A.z, A.w), g.mcy);
+                dz2 = __fadd2_rn(make_float2(B.x, B.y), g.mcz);
+                const float2 dd2 =
+                    __ffma2_rn(dx2, dx2, __ffma2_rn(dy2, dy2, __fmul2_rn(dz2, dz2)));
+                // shell entries beyond every site's cutoff (the list radius
+                // carries the region radius on top) add exactly nothing
+                if (MASK && dd2.x > g.out2) continue;
+                k0 = __fadd2_rn(dd2, g.oo02);
+                k1 = __fadd2_rn(dd2, g.oo12);
+                c12 = make_float2(T0.x, T0.y);
+                mc6 = make_float2(T0.z, T0.w);
+                m2c12 = make_float2(T1.x, T1.y);
+                c6 = make_float2(T1.z, T1.w);
+                if (MASK) {
+                    const float4 T2 = tq[2];
+                    sh = make_float2(T2.x, T2.y);
+                } else {
+                    fs += tq[2].x;
+                }
+                tp = T0;   // (unused on this path)
+            } else {
+                const float4 h = hb[e];
+                tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, -)
+                const float dx = h.x - g.cx, dy = h.y - g.cy, dz = h.z - g.cz;
+                const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                k0 = make_float2(dd + g.oo0, dd + g.oo0);
+                k1 = make_float2(dd + g.oo1, dd + g.oo1);
+                dx2 = make_float2(dx, dx);
+                dy2 = make_float2(dy, dy);
+                dz2 = make_float2(dz, dz);
+                c12 = make_float2(tp.x, tp.x);
+                c6 = make_float2(tp.y, tp.y);
+                sh = make_float2(tp.z, tp.z);
+                mc6 = make_float2(-tp.y, -tp.y);
+                m2c12 = make_float2(-2.f * tp.x, -2.f * tp.x);
+                if (!MASK) fs += tp.z;
+            }
 #pragma unroll
             for (int j = 0; j < PP; ++j) {
                 const float2 t =
@@ -509,8 +652,6 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
                     const float2 d2 = __ffma2_rn(q ? g.m1 : g.m0, t, q ? k1 : k0);
                     float2 fp;
                     if (RCP1) {
-                        const float2 mc6 = make_float2(-tp.y, -tp.y),
-                                     m2c12 = make_float2(-2.f * tp.x, -2.f * tp.x);
                         float r0, r1;
                         asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(d2.x));
                         asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r1) : "f"(d2.y));
@@ -524,6 +665,11 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
                                 make_float2(set_lt(d2.x, g.rc2f), set_lt(d2.y, g.rc2f));
                             n3 = __fmul2_rn(n3, m);
                             fe[j] = __ffma2_rn(m, sh, fe[j]);
+                            if (BORDER) {
+                                const float2 x = __fadd2_rn(d2, mrc2);
+                                border[2 * j] = fminf(border[2 * j], fabsf(x.x));
+                                border[2 * j + 1] = fminf(border[2 * j + 1], fabsf(x.y));
+                            }
                         }
                         fe[j] = __ffma2_rn(n3, __ffma2_rn(c12, n3, mc6), fe[j]);
                         fp = __fmul2_rn(__fmul2_rn(n1, n3), __ffma2_rn(m2c12, n3, c6));

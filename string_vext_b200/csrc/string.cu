@@ -10,6 +10,10 @@
 //      replaced by its first-order value g_k = h_k dE/dx_k (h = delta_frac for
 //      a, b, c and delta_angle for the angles; dE/dalpha = 0 exactly for a
 //      two-site guest), truncated as floor(g / 1e-15) 1e-15 (global.h:1281-1325);
+//      in the reference-difference mode the seven poses x, x + h_k e_k of
+//      every image are evaluated instead (one pose launch of 7 n poses, in the
+//      reference's variable order, remap_string_var, global.h:1141-1200) and
+//      g_k = E_k - E_0 is truncated the same way;
 //   2. step: per block (translation / rotation) L = |g| (truncated); if
 //      L < h: s1 = s0 - h g, else s1 = s0 - h trunc(g / L) (global.h:1347-1450);
 //   3. end fixing along the transport axis (global.h:1452-1620): image 0
@@ -56,6 +60,8 @@ struct StringArgs {
     double *lengths;      // [n] segment lengths, then cumulative
     int *flags;           // [0] stop, [1] conv_t, [2] conv_r, [3] iterations done
     double *totals;       // [0] translation movement, [1] rotation movement
+    int fd;               // reference one-sided differences instead of the adjoint
+    double *centers7, *quats7, *e7;   // [7n] poses x, x + h_k e_k and their energies
 };
 
 __device__ __forceinline__ double trunc_r(double x, double r) { return floor(x / r) * r; }
@@ -76,6 +82,24 @@ __global__ void string_to_pose_kernel(StringArgs a) {
         pose_of(a, a.s0 + 6 * i, a.centers + 3 * i, a.quats + 4 * i);
 }
 
+// The seven poses of image i for the reference's differences: variable 0 is
+// s0 itself, variable k = 1..6 adds h to coordinate k - 1 (delta_frac for
+// a, b, c; delta_angle for alpha, beta, gamma).  The director of a two-site
+// guest, R e_x = (cos g cos b, sin g cos b, -sin b), does not depend on
+// alpha, so the poses are built with alpha = 0: E(x + h e_alpha) - E(x) is
+// then exactly 0, as in the reference's own rotation.
+__global__ void string_fd_pose_kernel(StringArgs a) {
+    for (int v = threadIdx.x + blockIdx.x * blockDim.x; v < 7 * a.n;
+         v += blockDim.x * gridDim.x) {
+        const int i = v / 7, k = v % 7;
+        double s[6];
+        for (int c = 0; c < 6; ++c) s[c] = a.s0[6 * i + c];
+        if (k >= 1) s[k - 1] += k <= 3 ? a.hf : a.ha;
+        s[3] = 0.0;
+        pose_of(a, s, a.centers7 + 3 * v, a.quats7 + 4 * v);
+    }
+}
+
 // Steps 2-4 (and the pose of s2).  One CTA, thread i = image i (n <= 1024 =
 // blockDim): the step in registers, end fixing and segment lengths through
 // shared memory, the running sum of the lengths by one thread in image order.
@@ -90,16 +114,23 @@ __global__ void __launch_bounds__(1024) string_step_kernel(StringArgs a) {
     if (i < n) {
         const double *s = a.s0 + 6 * i;
         double g[6];
-        // dE/dfrac_k = sum_j H[k][j] dE/dcart_j
-        for (int k = 0; k < 3; ++k)
-            g[k] = a.hf * (a.H.m[3 * k] * a.gc[3 * i] + a.H.m[3 * k + 1] * a.gc[3 * i + 1] +
-                           a.H.m[3 * k + 2] * a.gc[3 * i + 2]);
-        // director u = (cg cb, sg cb, -sb); dE/dalpha = 0 for a linear guest
-        const double cb = cos(s[4]), sb = sin(s[4]), cg = cos(s[5]), sg = sin(s[5]);
-        const double *gu = a.gu + 3 * i;
-        g[3] = 0.0;
-        g[4] = a.ha * (gu[0] * (-cg * sb) + gu[1] * (-sg * sb) + gu[2] * (-cb));
-        g[5] = a.ha * (gu[0] * (-sg * cb) + gu[1] * (cg * cb));
+        if (a.fd) {
+            // s0_grad_cal, global.h:1281-1300: E(var k) - E(var 0)
+            const double *e7 = a.e7 + 7 * i;
+            for (int k = 0; k < 6; ++k) g[k] = e7[k + 1] - e7[0];
+            a.e0[i] = e7[0];
+        } else {
+            // dE/dfrac_k = sum_j H[k][j] dE/dcart_j
+            for (int k = 0; k < 3; ++k)
+                g[k] = a.hf * (a.H.m[3 * k] * a.gc[3 * i] + a.H.m[3 * k + 1] * a.gc[3 * i + 1] +
+                               a.H.m[3 * k + 2] * a.gc[3 * i + 2]);
+            // director u = (cg cb, sg cb, -sb); dE/dalpha = 0 for a linear guest
+            const double cb = cos(s[4]), sb = sin(s[4]), cg = cos(s[5]), sg = sin(s[5]);
+            const double *gu = a.gu + 3 * i;
+            g[3] = 0.0;
+            g[4] = a.ha * (gu[0] * (-cg * sb) + gu[1] * (-sg * sb) + gu[2] * (-cb));
+            g[5] = a.ha * (gu[0] * (-sg * cb) + gu[1] * (cg * cb));
+        }
         for (int k = 0; k < 6; ++k) g[k] = trunc_r(g[k], a.rounding);
         const double lt = trunc_r(sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]), a.rounding);
         const double lr = trunc_r(sqrt(g[3] * g[3] + g[4] * g[4] + g[5] * g[5]), a.rounding);
@@ -265,6 +296,7 @@ extern "C" void vext_string_default_params(vext_string_params *p) {
     p->conv_rot_percent = 30;
     p->max_iterations = 10000;
     p->check_every = 200;
+    p->gradient = VEXT_STRING_ANALYTIC;
 }
 
 extern "C" int vext_string_run(vext_system h, int n, double *path, double *energy,
@@ -275,7 +307,8 @@ extern "C" int vext_string_run(vext_system h, int n, double *path, double *energ
     vext_string_default_params(&p);
     if (params) p = *params;
     if (p.direction < 1 || p.direction > 3 || !(p.delta_frac > 0) || !(p.delta_angle_rad > 0) ||
-        p.max_iterations < 0 || p.check_every < 1)
+        p.max_iterations < 0 || p.check_every < 1 ||
+        (p.gradient != VEXT_STRING_ANALYTIC && p.gradient != VEXT_STRING_REFERENCE_FD))
         return fail(VEXT_ERR_ARGUMENT, "invalid String parameters");
     for (int k = 0; k < 6 * n; ++k)
         if (!std::isfinite(path[k])) return fail(VEXT_ERR_ARGUMENT, "non-finite path");
@@ -289,8 +322,9 @@ extern "C" int vext_string_run(vext_system h, int n, double *path, double *energ
     double *buf = nullptr;
     const size_t nd = (size_t)n;
     // s0 s1 s2 (6n each), e0 e2 lengths totals (n each), gc gu centers
-    // centers2 (3n each), quats quats2 (4n each)
-    const size_t words = 3 * 6 * nd + 4 * nd + 4 * 3 * nd + 2 * 4 * nd;
+    // centers2 (3n each), quats quats2 (4n each), centers7 quats7 e7 (21n,
+    // 28n, 7n)
+    const size_t words = 3 * 6 * nd + 4 * nd + 4 * 3 * nd + 2 * 4 * nd + 56 * nd;
     VEXT_CUDA(cudaMalloc(&buf, sizeof(double) * words));
     int *flags = nullptr;
     cudaError_t e = cudaMalloc(&flags, sizeof(int) * 8);
@@ -322,6 +356,10 @@ extern "C" int vext_string_run(vext_system h, int n, double *path, double *energ
     a.quats = q; q += 4 * nd;
     a.centers2 = q; q += 3 * nd;
     a.quats2 = q; q += 4 * nd;
+    a.centers7 = q; q += 21 * nd;
+    a.quats7 = q; q += 28 * nd;
+    a.e7 = q; q += 7 * nd;
+    a.fd = p.gradient == VEXT_STRING_REFERENCE_FD;
     if ((size_t)(q - buf) != words) {   // the carve-out must match the allocation exactly
         cudaFree(buf);
         cudaFree(flags);
@@ -336,7 +374,15 @@ extern "C" int vext_string_run(vext_system h, int n, double *path, double *energ
         VEXT_CUDA(cudaGetLastError());
         // one iteration = two pose evaluations + two single-CTA kernels
         auto iteration = [&](int check) -> int {
-            VEXT_TRY(pose_enqueue(sys, n, a.centers, a.quats, o, a.e0, a.gc, nullptr, a.gu, st));
+            if (a.fd) {
+                string_fd_pose_kernel<<<(7 * n + 255) / 256, 256, 0, st>>>(a);
+                VEXT_CUDA(cudaGetLastError());
+                VEXT_TRY(pose_enqueue(sys, 7 * n, a.centers7, a.quats7, o, a.e7, nullptr, nullptr,
+                                      nullptr, st));
+            } else {
+                VEXT_TRY(pose_enqueue(sys, n, a.centers, a.quats, o, a.e0, a.gc, nullptr, a.gu,
+                                      st));
+            }
             string_step_kernel<<<1, 1024, 0, st>>>(a);
             VEXT_CUDA(cudaGetLastError());
             VEXT_TRY(pose_enqueue(sys, n, a.centers2, a.quats2, o, a.e2, nullptr, nullptr,

@@ -552,6 +552,22 @@ extern "C" int vext_system_create(const vext_system_desc *d, vext_system *out) {
         }
     }
     s.n_types = (int)ids.size();
+    {
+        uint64_t hsh = 1469598103934665603ull;
+        auto mix = [&hsh](const void *p, size_t n) {
+            const unsigned char *c = static_cast<const unsigned char *>(p);
+            for (size_t i = 0; i < n; ++i) hsh = (hsh ^ c[i]) * 1099511628211ull;
+        };
+        mix(h, 9 * sizeof(double));
+        mix(&d->cutoff, sizeof(double));
+        mix(&s.n_atoms, sizeof(int));
+        mix(frac.data(), frac.size() * sizeof(double));
+        mix(type.data(), type.size() * sizeof(int));
+        std::vector<std::pair<double, double>> by_id(ids.size());
+        for (auto &kv : ids) by_id[kv.second] = kv.first;
+        mix(by_id.data(), by_id.size() * sizeof(by_id[0]));
+        s.frame_hash = hsh;
+    }
     if (s.n_types > kMaxTypes) {
         delete handle;
         return fail(VEXT_ERR_CAPACITY, "%d distinct framework (sigma, epsilon) pairs; limit %d",

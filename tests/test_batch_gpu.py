@@ -3,7 +3,11 @@ through the C ABI: each system's output equals its own single-field
 mixed-precision result on the same region size bit for bit (same lists,
 same pair loops, same order) -- 8-center regions, the batch default, and 16,
 the single-field default -- agrees with the FP64 kernel within the stated
-tolerance, and replays reproduce it."""
+tolerance, and replays reproduce it.  The two guests of one framework share
+one region-list set, built for the guest with the larger site offset; the
+other guest's results then come from lists with a wider near class and a
+longer list, so they match its single-field result within the precision bar
+rather than bit for bit."""
 import numpy as np
 import pytest
 import torch
@@ -13,6 +17,17 @@ from string_vext_b200.orientation import normalized_directors, regular_pose_grid
 from string_vext_b200.system import VextBatch, VextSystem
 
 pytestmark = pytest.mark.gpu
+
+
+def list_owner(k, n_frameworks):
+    """Batch systems 2f, 2f + 1 are framework f with guests A (bond 1.54 A)
+    and B (bond 1.33 A): A's larger offset builds the shared lists."""
+    return k >= 2 * n_frameworks or k % 2 == 0
+
+
+def assert_close_to(got, single):
+    diff = np.abs(got.astype(np.float64) - single.astype(np.float64))
+    assert (diff <= 2e-4 + 2e-6 * np.abs(single.astype(np.float64))).all()
 
 
 def test_batch_matches_single_fields():
@@ -30,9 +45,12 @@ def test_batch_matches_single_fields():
         batch16.run()
         batch16.check()
         torch.cuda.synchronize()
-        for case, system, out in zip(cases, systems, outs16):
+        for k, (system, out) in enumerate(zip(systems, outs16)):
             single = system.field(size, axes)["orientation_K"]     # 16-center regions
-            np.testing.assert_array_equal(out.cpu().numpy(), single)
+            if list_owner(k, 3):
+                np.testing.assert_array_equal(out.cpu().numpy(), single)
+            else:
+                assert_close_to(out.cpu().numpy(), single)
     batch16.close()
     outs = [torch.full((64, size, size, size), -1.0, dtype=torch.float32, device="cuda")
             for _ in systems]
@@ -51,9 +69,12 @@ def test_batch_matches_single_fields():
             first = got
         for a, b in zip(first, got):
             np.testing.assert_array_equal(a, b)
-        for system, out in zip(systems, got):
+        for k, (system, out) in enumerate(zip(systems, got)):
             single = system.field(size, axes, centers_per_region=8)["orientation_K"]
-            np.testing.assert_array_equal(out, single)
+            if list_owner(k, 3):
+                np.testing.assert_array_equal(out, single)
+            else:
+                assert_close_to(out, single)
     for case, system, out in zip(cases, systems, outs):
         exact = system.field(size, axes, mode=_lib.VEXT_MODE_FP64, energy=True,
                              orientation=False)["energy"].T.reshape(64, size, size, size)
@@ -66,5 +87,25 @@ def test_batch_matches_single_fields():
         if (~neg).any():
             assert ((np.abs(got - exact) - ulp) / np.maximum(np.abs(exact), 1))[~neg].max() < 1e-6
     batch.close()
+    for s in systems:
+        s.close()
+
+
+def test_guests_of_one_framework_share_their_lists():
+    """Two guests of one framework hold one list set: the batch's list memory
+    is that of the larger-offset guest alone."""
+    cases = synth.batch_frameworks(1)
+    size = 6
+    _, axes = regular_pose_grid(size, 64)
+    axes = normalized_directors(axes)
+    systems = [VextSystem(c) for c in cases]
+    shape = (64, size, size, size)
+    both = VextBatch(systems, size, axes,
+                     [torch.empty(shape, dtype=torch.float32, device="cuda") for _ in systems])
+    alone = VextBatch(systems[:1], size, axes,
+                      [torch.empty(shape, dtype=torch.float32, device="cuda")])
+    assert both.info()["list_bytes"] == alone.info()["list_bytes"] > 0
+    both.close()
+    alone.close()
     for s in systems:
         s.close()

@@ -141,13 +141,21 @@ def test_adjoint_batch_matches_single_fields_and_host_entry():
         batch.run()
         batch.check()
         torch.cuda.synchronize()
-        for system, out, grad in zip(systems, outs, grads):
+        for k, (system, out, grad) in enumerate(zip(systems, outs, grads)):
             e, g = system.field_adjoint(size, axes)
-            np.testing.assert_array_equal(out.cpu().numpy(), e)
-            np.testing.assert_array_equal(grad.cpu().numpy(), g)
             de, dg = run_device(system, size, axes, MIXED)
             np.testing.assert_array_equal(de, e)
             np.testing.assert_array_equal(dg, g)
+            if k >= 4 or k % 2 == 0:    # the owner of its framework's shared lists
+                np.testing.assert_array_equal(out.cpu().numpy(), e)
+                np.testing.assert_array_equal(grad.cpu().numpy(), g)
+            else:                       # guest B on guest A's lists: within the bar
+                got, ge = out.cpu().numpy().astype(np.float64), e.astype(np.float64)
+                assert (np.abs(got - ge) <= 2e-4 + 2e-6 * np.abs(ge)).all()
+                gg, gs = grad.cpu().numpy().astype(np.float64), g.astype(np.float64)
+                rel = (np.linalg.norm(gg - gs, axis=-1)
+                       / np.maximum(np.linalg.norm(gs, axis=-1), 1.0))
+                assert rel.max() < 2e-5
     batch.close()
     for s in systems:
         s.close()
@@ -340,3 +348,43 @@ def test_director_reversal_at_full_size():
         assert ((ga[..., :3] - gb[..., :3]).norm(dim=-1) / scale).max().item() < 2e-5
         scale = ga[..., 3:].norm(dim=-1).clamp(min=1.0)
         assert ((ga[..., 3:] + gb[..., 3:]).norm(dim=-1) / scale).max().item() < 2e-5
+
+
+def test_batch_frameworks_gradients_within_bar_for_every_pose():
+    """The first 24 systems of the batched workload (12 seeded frameworks x
+    both guests, uneven cells and atom counts), 12^3 x 64 poses each (2.65 M
+    poses) through one forward + adjoint batch: every pose's gradient within
+    1e-5 (norm relative to max(|grad E|, 1 K/A)) of the plain FP64 adjoint,
+    energies within the bar.  A shell pair within FP32 rounding of the cutoff
+    would move a gradient by the force jump at rc (about 0.05 K/A); such
+    poses are re-evaluated in FP64, so no pose may exceed the bar."""
+    cases = synth.batch_frameworks(12)
+    size = 12
+    _, axes = regular_pose_grid(size, 64)
+    axes = normalized_directors(axes)
+    systems = [VextSystem(c) for c in cases]
+    shape = (64, size, size, size)
+    outs = [torch.empty(shape, dtype=torch.float32, device="cuda") for _ in systems]
+    grads = [torch.empty(shape + (6,), dtype=torch.float32, device="cuda") for _ in systems]
+    batch = VextBatch(systems, size, axes, outs, gradients=grads)
+    batch.run()
+    batch.check()
+    torch.cuda.synchronize()
+    worst = 0.0
+    for system, out, grad in zip(systems, outs, grads):
+        e64 = torch.empty(shape, dtype=torch.float64, device="cuda")
+        g64 = torch.empty(shape + (6,), dtype=torch.float64, device="cuda")
+        system.field_adjoint_device(size, axes, None, None, e64, g64,
+                                    mode=_lib.VEXT_MODE_FP64_PLAIN)
+        torch.cuda.synchronize()
+        ex, gx = e64.cpu().numpy(), g64.cpu().numpy()
+        got = out.cpu().numpy().astype(np.float64)
+        # float32 storage: compare the energies at float32 resolution
+        assert (np.abs(got - ex) <= 1e-4 + 1.2e-7 * np.abs(ex)).all()
+        gm = grad.cpu().numpy().astype(np.float64)
+        grel = np.linalg.norm(gm - gx, axis=-1) / np.maximum(np.linalg.norm(gx, axis=-1), 1.0)
+        worst = max(worst, float(grel.max()))
+    batch.close()
+    for s in systems:
+        s.close()
+    assert worst < 1e-5, f"worst gradient error {worst}"
