@@ -44,6 +44,7 @@ struct RegionSet {
     // key
     int size = 0, bi = 0, bj = 0, bk = 0;   // field regions (size > 0) or bins (size == 0)
     int nb[3] = {0, 0, 0};                  // bins per axis (pose regions)
+    double bin_width = 0;                   // target bin width (A, pose regions)
     double r_split = 0;
     // data
     int n_regions = 0;
@@ -157,7 +158,9 @@ int batch_retarget(vext_batch b, int k, float *out, float *grad, cudaStream_t st
 // Region sets (system.cu)
 int get_field_regions(System *sys, int size, int cb, double r_split, RegionSet **out,
                       cudaStream_t stream);
-int get_bin_regions(System *sys, double r_split, RegionSet **out, cudaStream_t stream);
+constexpr double kBinWidth = 1.5;   // default pose-bin width between lattice planes (A)
+int get_bin_regions(System *sys, double r_split, RegionSet **out, cudaStream_t stream,
+                    double bin_width = kBinWidth);
 void choose_block_shape(const Mat3 &H, int size, int cb, int &bi, int &bj, int &bk);
 double block_radius(const Mat3 &H, int size, int ni, int nj, int nk);
 

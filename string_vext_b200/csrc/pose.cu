@@ -23,6 +23,9 @@ namespace vext {
 constexpr int kPoseThreads = 128;
 // vext_options.variant bit: the far loop on expanded entries (far_expand)
 constexpr int kPoseVariantX2 = 4096;
+// bins of 1.0 A or 0.75 A instead of kBinWidth
+constexpr int kPoseVariantBin100 = 8192;
+constexpr int kPoseVariantBin075 = 16384;
 
 struct PoseArgs {
     Mat3 H, Hinv;
@@ -494,7 +497,9 @@ int pose_enqueue(System *sys, int n, const double *centers, const double *quats,
         return fail(VEXT_ERR_ARGUMENT, "unknown precision mode %d", o.mode);
     const double r_split = o.mode == VEXT_MODE_FP64 ? 1e30 : o.r_split;
     RegionSet *rs = nullptr;
-    VEXT_TRY(get_bin_regions(sys, r_split, &rs, st));
+    const double width = o.variant & kPoseVariantBin100 ? 1.0
+                         : o.variant & kPoseVariantBin075 ? 0.75 : kBinWidth;
+    VEXT_TRY(get_bin_regions(sys, r_split, &rs, st, width));
     const int n_bins = rs->n_regions;
     // Fewer than 64 poses per bin on average: the binned pipeline would give
     // most of its per-bin CTAs a handful of poses for a whole list each; one

@@ -364,11 +364,11 @@ int get_field_regions(System *sys, int size, int cb, double r_split, RegionSet *
 }
 
 // Width (A, between lattice planes) of the pose bins.
-constexpr double kBinWidth = 1.5;
 
-int get_bin_regions(System *sys, double r_split, RegionSet **out, cudaStream_t stream) {
+int get_bin_regions(System *sys, double r_split, RegionSet **out, cudaStream_t stream,
+                    double bin_width) {
     for (RegionSet *rs : sys->sets)
-        if (rs->size == 0 && rs->r_split == r_split) {
+        if (rs->size == 0 && rs->r_split == r_split && rs->bin_width == bin_width) {
             if (rs->stale) {
                 for (auto &r : rs->h_info) r.n_near = r.n_total = r.n_inner = 0;
                 VEXT_TRY(build_lists(sys, rs, stream));
@@ -378,9 +378,10 @@ int get_bin_regions(System *sys, double r_split, RegionSet **out, cudaStream_t s
         }
     RegionSet *rs = new RegionSet();
     rs->r_split = r_split;
-    // Bins about kBinWidth wide between lattice planes.
+    rs->bin_width = bin_width;
+    // Bins about bin_width wide between lattice planes.
     for (int k = 0; k < 3; ++k)
-        rs->nb[k] = std::max(1, (int)std::ceil((1.0 / sys->einv[k]) / kBinWidth));
+        rs->nb[k] = std::max(1, (int)std::ceil((1.0 / sys->einv[k]) / bin_width));
     rs->n_ri = rs->nb[0];
     rs->n_rj = rs->nb[1];
     rs->n_rk = rs->nb[2];

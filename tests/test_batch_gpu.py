@@ -109,3 +109,32 @@ def test_guests_of_one_framework_share_their_lists():
     alone.close()
     for s in systems:
         s.close()
+
+
+def test_autotuner_pick_is_cached_per_size_class():
+    """A batch timed afresh (variant bit 2048) stores its pick; the next batch
+    of the same kernel table and size class reuses it without timing runs
+    (same pick, the stored sample times), and both give the same bits."""
+    case = synth.small_field()
+    size = 5
+    _, axes = regular_pose_grid(size, 64)
+    axes = normalized_directors(axes)
+    shape = (64, size, size, size)
+    with VextSystem(case) as system:
+        outs = []
+        infos = []
+        for variant in (2048, 0):
+            e = torch.empty(shape, dtype=torch.float32, device="cuda")
+            g = torch.empty(shape + (6,), dtype=torch.float32, device="cuda")
+            batch = VextBatch([system], size, axes, [e], gradients=[g], variant=variant)
+            batch.run()
+            batch.check()
+            torch.cuda.synchronize()
+            infos.append(batch.info())
+            outs.append((e.cpu().numpy(), g.cpu().numpy()))
+            batch.close()
+        assert (infos[0]["shape"], infos[0]["grid"]) == (infos[1]["shape"], infos[1]["grid"])
+        assert ([t["sample_ms"] for t in infos[0]["tuning"]]
+                == [t["sample_ms"] for t in infos[1]["tuning"]])
+        np.testing.assert_array_equal(outs[0][0], outs[1][0])
+        np.testing.assert_array_equal(outs[0][1], outs[1][1])
