@@ -141,7 +141,7 @@ enum {
 
 typedef struct {
     int mode;                /* VEXT_MODE_*                                   */
-    double r_split;          /* A; <= 0 selects the default (6 A)             */
+    double r_split;          /* A; <= 0 selects the default (5 A)             */
     double band_lo, band_hi; /* refinement band for E (K); band_hi <= band_lo
                                 disables refinement; defaults via
                                 vext_default_options                          */

@@ -74,17 +74,14 @@ struct BatchArgs {
 // BORDER: border[p] receives the smallest |q - rc^2| (FP32) of director p
 // over the masked shell pairs, for the FP64 re-evaluation of poses with a
 // pair too close to the cutoff for the FP32 test.
-// X2: far chunks are expanded in shared memory (far_expand, into the near
-// conversion buffer ed) and read with the pre-paired type table stx.
 template <int CB, int G, int P, bool NEWTON, bool RCP1, int UNROLL, int FLUSH, bool GSUM,
-          bool BORDER, bool X2>
+          bool BORDER>
 __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSys &y,
                                                const RegionInfo &r, Stager &st, double *ed,
                                                const float4 *stf, const double *std4,
-                                               double *gsum, const float4 *stx, unsigned &seq,
-                                               double cx, double cy, double cz, int obase,
-                                               double (&e)[P], double (&gr)[P][6],
-                                               float (&border)[P]) {
+                                               double *gsum, unsigned &seq, double cx,
+                                               double cy, double cz, int obase, double (&e)[P],
+                                               double (&gr)[P][6], float (&border)[P]) {
     constexpr int NT = CB * G, PP = P / 2;
     AdjAcc acc[P];
     adj_zero(acc);
@@ -185,20 +182,12 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
                 plan.chunk(c, start, len, near);
                 const float4 *hb = st.hib + ((seq + c) % kStages) * kCH;
                 constexpr int GNT = GSUM ? NT : 0;
-                const float4 *tab = stf;
-                if constexpr (X2) {
-                    float4 *xb = reinterpret_cast<float4 *>(ed);
-                    far_expand<NT>(hb, xb, len);
-                    __syncthreads();
-                    hb = xb;
-                    tab = stx;
-                }
                 if (pass)
-                    far_chunk_adj<P, NEWTON, FLUSH, true, RCP1, UNROLL, GNT, BORDER, X2>(
-                        hb, tab, len, g, ux, uy, uz, acc, shift_sum, gsum, border);
+                    far_chunk_adj<P, NEWTON, FLUSH, true, RCP1, UNROLL, GNT, BORDER>(
+                        hb, stf, len, g, ux, uy, uz, acc, shift_sum, gsum, border);
                 else
-                    far_chunk_adj<P, NEWTON, FLUSH, false, RCP1, UNROLL, GNT, false, X2>(
-                        hb, tab, len, g, ux, uy, uz, acc, shift_sum, gsum);
+                    far_chunk_adj<P, NEWTON, FLUSH, false, RCP1, UNROLL, GNT>(
+                        hb, stf, len, g, ux, uy, uz, acc, shift_sum, gsum);
                 stage_next(st, plan, y.hi, y.lo, c, seq);
             }
             seq += plan.n_chunks;
@@ -220,8 +209,7 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
 // 5 = as 1 with the far entry loop unrolled twice; 6 / 7 = as 1 with the
 // FP32 gradient partials flushed every 16 / 64 entries instead of once per
 // 128-entry chunk; 8 = as 1 with the FP64 gradient sums in shared memory
-// during the far passes (fewer registers: more resident CTAs); 9 / 10 = as
-// 8 / 1 with the far chunks expanded in shared memory (far_expand).
+// during the far passes (fewer registers: more resident CTAs).
 template <int CB, int G, int P, int MINB, int ADJ, bool BORDER = false>
 __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
     constexpr int NT = CB * G, PP = P / 2;
@@ -234,7 +222,7 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
     double *ed = reinterpret_cast<double *>(st.lob + kStages * kCH);   // [kCH][4]
     float4 *stf = reinterpret_cast<float4 *>(ed + 4 * kCH);
     const int tid = threadIdx.x;
-    constexpr bool kX2 = ADJ == 9 || ADJ == 10, kGsum = ADJ == 8 || ADJ == 9;
+    constexpr bool kGsum = ADJ == 8;
     init_barriers(st);
     int last_sys = -1;
     unsigned seq = 0;
@@ -246,11 +234,8 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
         const int4 w = a.items[it];
         const BatchSys &y = a.sys[w.x];
         double *std4 = reinterpret_cast<double *>(stf + y.n_types);
-        // behind the gradient sums: the pre-paired type table (kX2)
-        float4 *stx = reinterpret_cast<float4 *>(std4 + 4 * y.n_types + kGradWords * 512);
         if (w.x != last_sys) {
             load_types<NT>(stf, std4, y.tf, y.td, y.n_types);
-            if constexpr (kX2) far_types_x2<NT>(stx, y.tf, y.n_types);
             last_sys = w.x;
         }
         __syncthreads();
@@ -271,8 +256,8 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
             double *gsum = reinterpret_cast<double *>(std4 + 4 * y.n_types);
             if (!batch_item_adj<CB, G, P, ADJ == 2, ADJ == 1 || ADJ >= 5,
                                 ADJ == 5 ? 2 : 1, ADJ == 6 ? 16 : ADJ == 7 ? 64 : 128,
-                                kGsum, BORDER, kX2>(a, y, r, st, ed, stf, std4, gsum, stx, seq,
-                                                    cx, cy, cz, obase, e, gr, border))
+                                kGsum, BORDER>(a, y, r, st, ed, stf, std4, gsum, seq, cx, cy,
+                                               cz, obase, e, gr, border))
                 return;
         } else {
         // ---- near pairs (FP64)
@@ -517,9 +502,7 @@ static const BatchKernel kForwardCb8Kernels[] = {
 static const BatchKernel kAdjointCb8Kernels[] = {
     {batch_field_kernel<8, 16, 4, 3, 8, true>, 128, "8c 128x4/3 gsum"},
     {batch_field_kernel<8, 16, 4, 2, 1, true>, 128, "8c 128x4"},
-    {batch_field_kernel<8, 32, 2, 2, 1, true>, 256, "8c 256x2"},
-    {batch_field_kernel<8, 16, 4, 3, 9, true>, 128, "8c 128x4/3 gsum x2"},
-    {batch_field_kernel<8, 16, 4, 2, 10, true>, 128, "8c 128x4 x2"}};
+    {batch_field_kernel<8, 32, 2, 2, 1, true>, 256, "8c 256x2"}};
 // the same without the cutoff-border test (timing study: its cost)
 static const BatchKernel kAdjointCb8NoBorderKernels[] = {
     {batch_field_kernel<8, 16, 4, 3, 8>, 128, "8c 128x4/3 gsum, no border test"},
@@ -629,7 +612,7 @@ struct vext_batch_s {
 // 16 centers x 32 directors for the adjoint kernels that park them there).
 static size_t batch_smem(int max_types, bool adj) {
     return kStageBytes + (size_t)kCH * 4 * sizeof(double) + (size_t)max_types * 48 +
-           (adj ? (size_t)kGradWords * 16 * 32 * sizeof(double) + (size_t)max_types * 48 : 0);
+           (adj ? (size_t)kGradWords * 16 * 32 * sizeof(double) : 0);
 }
 
 static int batch_launch(vext_batch b, const BatchConfig &cfg, const int4 *items, int n_items,

@@ -24,7 +24,7 @@
 namespace vext {
 
 constexpr int kMaxTypes = 1024;     // distinct framework (sigma, epsilon) pairs
-constexpr double kDefaultRSplit = 6.0;
+constexpr double kDefaultRSplit = 5.0;
 
 struct alignas(16) RegionInfo {
     double of[3];       // origin, fractional
@@ -158,7 +158,7 @@ int batch_retarget(vext_batch b, int k, float *out, float *grad, cudaStream_t st
 // Region sets (system.cu)
 int get_field_regions(System *sys, int size, int cb, double r_split, RegionSet **out,
                       cudaStream_t stream);
-constexpr double kBinWidth = 1.5;   // default pose-bin width between lattice planes (A)
+constexpr double kBinWidth = 0.75;  // pose-bin width between lattice planes (A)
 int get_bin_regions(System *sys, double r_split, RegionSet **out, cudaStream_t stream,
                     double bin_width = kBinWidth);
 void choose_block_shape(const Mat3 &H, int size, int cb, int &bi, int &bj, int &bk);

@@ -244,8 +244,6 @@ struct FarGeom {
     float2 m0, m1;             // -2 o_s, broadcast
     float oo0, oo1;            // o_s^2
     float rc2f;
-    float2 mcx, mcy, mcz;      // -c, broadcast (expanded entries)
-    float2 oo02, oo12;         // o_s^2, broadcast (expanded entries)
     float out2;                // |d0|^2 beyond which no site of the pose reaches rc
 };
 
@@ -260,42 +258,11 @@ __device__ __forceinline__ FarGeom far_geom(double cxd, double cyd, double czd, 
     g.oo0 = (float)(off0 * off0);
     g.oo1 = (float)(off1 * off1);
     g.rc2f = rc2f;
-    g.mcx = make_float2(-g.cx, -g.cx);
-    g.mcy = make_float2(-g.cy, -g.cy);
-    g.mcz = make_float2(-g.cz, -g.cz);
-    g.oo02 = make_float2(g.oo0, g.oo0);
-    g.oo12 = make_float2(g.oo1, g.oo1);
     // (rc + max|o| + 1e-3 A)^2: a site is at least |d0| - max|o| from the
     // entry, so beyond this every pair is out by far more than FP32 rounding
     const double rmax = sqrt((double)rc2f) + fmax(fabs(off0), fabs(off1)) + 1e-3;
     g.out2 = (float)(rmax * rmax);
     return g;
-}
-
-// Expanded far entries: the packed FP32x2 loops take each scalar of an entry
-// as a (v, v) pair, so a staged chunk of (x, y, z, type) entries is rewritten
-// once per CTA as two float4 (x, x, y, y), (z, z, type, 0) that load straight
-// into register pairs; the pair coefficients of every type wait pre-paired in
-// the same way (far_types_x2).  The arithmetic and its rounding are those of
-// the scalar entries.
-template <int NT>
-__device__ __forceinline__ void far_expand(const float4 *hb, float4 *xb, int len) {
-    for (int e = threadIdx.x; e < len; e += NT) {
-        const float4 h = hb[e];
-        xb[2 * e] = make_float4(h.x, h.x, h.y, h.y);
-        xb[2 * e + 1] = make_float4(h.z, h.z, h.w, 0.f);
-    }
-}
-
-// Per type: (c12, c12, -c6, -c6), (-2 c12, -2 c12, c6, c6), (shift, shift, shift, 0).
-template <int NT>
-__device__ __forceinline__ void far_types_x2(float4 *stx, const float4 *tf, int n_types) {
-    for (int t = threadIdx.x; t < n_types; t += NT) {
-        const float4 p = tf[t];
-        stx[3 * t] = make_float4(p.x, p.x, -p.y, -p.y);
-        stx[3 * t + 1] = make_float4(-2.f * p.x, -2.f * p.x, p.y, p.y);
-        stx[3 * t + 2] = make_float4(p.z, p.z, p.z, 0.f);
-    }
 }
 
 // The earlier forward far chunk, kept for comparison with far_chunk_fwd:
@@ -360,7 +327,9 @@ __device__ __forceinline__ void far_chunk(const float4 *hb, const float4 *stf, i
 // Newton step), n3 = n1^3 = q^-3, e = n3 (c12 n3 - c6); MASK as in
 // far_chunk_adj (inner entries: no mask, shift summed once per entry into
 // shift_sum, to be added twice -- both sites -- to every energy).  FP32
-// partials over FLUSH entries are flushed into the FP64 acc.
+// partials over FLUSH entries are flushed into the FP64 acc.  Shell entries
+// beyond every site's cutoff (the list radius carries the region radius on
+// top) are skipped: they would add exactly nothing.
 template <int P, int FLUSH, bool MASK>
 __device__ __forceinline__ void far_chunk_fwd(const float4 *hb, const float4 *stf, int len,
                                               const FarGeom &g, const float2 (&ux)[P / 2],
@@ -377,17 +346,23 @@ __device__ __forceinline__ void far_chunk_fwd(const float4 *hb, const float4 *st
         const int e1 = min(e0 + FLUSH, len);
 #pragma unroll 2
         for (int e = e0; e < e1; ++e) {
-            const float4 h = hb[e];
-            const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, -)
-            const float dx = h.x - g.cx, dy = h.y - g.cy, dz = h.z - g.cz;
-            const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            const float2 k0 = make_float2(dd + g.oo0, dd + g.oo0),
-                         k1 = make_float2(dd + g.oo1, dd + g.oo1);
-            const float2 dx2 = make_float2(dx, dx), dy2 = make_float2(dy, dy),
-                         dz2 = make_float2(dz, dz);
-            const float2 c12 = make_float2(tp.x, tp.x), mc6 = make_float2(-tp.y, -tp.y),
-                         sh = make_float2(tp.z, tp.z);
-            if (!MASK) fs += tp.z;
+            float2 k0, k1, dx2, dy2, dz2, c12, mc6, sh;
+            {
+                const float4 h = hb[e];
+                const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, -)
+                const float dx = h.x - g.cx, dy = h.y - g.cy, dz = h.z - g.cz;
+                const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                if (MASK && dd > g.out2) continue;
+                k0 = make_float2(dd + g.oo0, dd + g.oo0);
+                k1 = make_float2(dd + g.oo1, dd + g.oo1);
+                dx2 = make_float2(dx, dx);
+                dy2 = make_float2(dy, dy);
+                dz2 = make_float2(dz, dz);
+                c12 = make_float2(tp.x, tp.x);
+                mc6 = make_float2(-tp.y, -tp.y);
+                sh = make_float2(tp.z, tp.z);
+                if (!MASK) fs += tp.z;
+            }
 #pragma unroll
             for (int j = 0; j < PP; ++j) {
                 const float2 t =
@@ -565,10 +540,10 @@ __device__ __forceinline__ void grad_load(double *gsum, AdjAcc (&acc)[P]) {
 // the cutoff for the FP32 test to decide it like the FP64 one can be
 // re-evaluated in FP64 (the force jumps at rc, so a pair counted on the
 // other side moves the gradient by the jump).
-// X2: hb holds expanded entries (far_expand) and stf the pre-paired type
-// table (far_types_x2); same results, fewer instructions per entry.
+// Shell entries beyond every site's cutoff are skipped (they add exactly
+// nothing).
 template <int P, bool NEWTON, int FLUSH, bool MASK, bool RCP1 = true, int UNROLL = 1,
-          int GSUM_NT = 0, bool BORDER = false, bool X2 = false>
+          int GSUM_NT = 0, bool BORDER = false>
 __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *stf, int len,
                                               const FarGeom &g, const float2 (&ux)[P / 2],
                                               const float2 (&uy)[P / 2],
@@ -601,36 +576,12 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
         for (int e = b0; e < b1; ++e) {
             float2 k0, k1, dx2, dy2, dz2, c12, c6, sh, mc6, m2c12;
             float4 tp;
-            if constexpr (X2) {
-                const float4 A = hb[2 * e], B = hb[2 * e + 1];
-                const float4 *tq = stf + 3 * __float_as_int(B.z);
-                const float4 T0 = tq[0], T1 = tq[1];
-                dx2 = __fadd2_rn(make_float2(A.x, A.y), g.mcx);
-                dy2 = __fadd2_rn(make_float2(A.z, A.w), g.mcy);
-                dz2 = __fadd2_rn(make_float2(B.x, B.y), g.mcz);
-                const float2 dd2 =
-                    __ffma2_rn(dx2, dx2, __ffma2_rn(dy2, dy2, __fmul2_rn(dz2, dz2)));
-                // shell entries beyond every site's cutoff (the list radius
-                // carries the region radius on top) add exactly nothing
-                if (MASK && dd2.x > g.out2) continue;
-                k0 = __fadd2_rn(dd2, g.oo02);
-                k1 = __fadd2_rn(dd2, g.oo12);
-                c12 = make_float2(T0.x, T0.y);
-                mc6 = make_float2(T0.z, T0.w);
-                m2c12 = make_float2(T1.x, T1.y);
-                c6 = make_float2(T1.z, T1.w);
-                if (MASK) {
-                    const float4 T2 = tq[2];
-                    sh = make_float2(T2.x, T2.y);
-                } else {
-                    fs += tq[2].x;
-                }
-                tp = T0;   // (unused on this path)
-            } else {
+            {
                 const float4 h = hb[e];
                 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, -)
                 const float dx = h.x - g.cx, dy = h.y - g.cy, dz = h.z - g.cz;
                 const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                if (MASK && dd > g.out2) continue;
                 k0 = make_float2(dd + g.oo0, dd + g.oo0);
                 k1 = make_float2(dd + g.oo1, dd + g.oo1);
                 dx2 = make_float2(dx, dx);

@@ -21,11 +21,7 @@
 namespace vext {
 
 constexpr int kPoseThreads = 128;
-// vext_options.variant bit: the far loop on expanded entries (far_expand)
-constexpr int kPoseVariantX2 = 4096;
-// bins of 1.0 A or 0.75 A instead of kBinWidth
-constexpr int kPoseVariantBin100 = 8192;
-constexpr int kPoseVariantBin075 = 16384;
+
 
 struct PoseArgs {
     Mat3 H, Hinv;
@@ -189,9 +185,7 @@ __device__ __forceinline__ void write_pose(const PoseArgs &a, int p, double e, c
 // cutoff mask, and the shift is summed once per entry into shift_sum (added
 // to both sites).  Energy partials are flushed into FP64 every 16 entries,
 // the gradient partials once per call.
-// X2: hb holds expanded entries (far_expand) and stf the pre-paired type
-// table (far_types_x2): the same arithmetic without broadcasting scalars.
-template <bool MASK, bool X2 = false>
+template <bool MASK>
 __device__ __forceinline__ void pose_far(const float4 *hb, const float4 *stf, int e_begin,
                                          int e_end, float2 nsx, float2 nsy, float2 nsz,
                                          float rc2f, double (&E)[2], double (&F)[2][3],
@@ -205,24 +199,7 @@ __device__ __forceinline__ void pose_far(const float4 *hb, const float4 *stf, in
 #pragma unroll 2
         for (int e = e0; e < e1; ++e) {
             float2 dx, dy, dz, c12, mc6, m2c12, c6, sh;
-            if constexpr (X2) {
-                const float4 A = hb[2 * e], B = hb[2 * e + 1];
-                const float4 *tq = stf + 3 * __float_as_int(B.z);
-                const float4 T0 = tq[0], T1 = tq[1];
-                dx = __fadd2_rn(make_float2(A.x, A.y), nsx);
-                dy = __fadd2_rn(make_float2(A.z, A.w), nsy);
-                dz = __fadd2_rn(make_float2(B.x, B.y), nsz);
-                c12 = make_float2(T0.x, T0.y);
-                mc6 = make_float2(T0.z, T0.w);
-                m2c12 = make_float2(T1.x, T1.y);
-                c6 = make_float2(T1.z, T1.w);
-                if (MASK) {
-                    const float4 T2 = tq[2];
-                    sh = make_float2(T2.x, T2.y);
-                } else {
-                    fs += tq[2].x;
-                }
-            } else {
+            {
                 const float4 h = hb[e];
                 const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, floor2)
                 dx = __fadd2_rn(make_float2(h.x, h.x), nsx);
@@ -269,7 +246,7 @@ __device__ __forceinline__ void pose_far(const float4 *hb, const float4 *stf, in
 // (the FP64 mode: every entry is near) the correctly rounded reciprocal.
 // NEAR_IN: the host proved every near pair inside the cutoff (r_split + 2
 // (rho + max|offset|) < rc), so near pairs skip the cutoff test.
-template <int NT, bool MIXED, bool NEAR_IN, bool X2 = false>
+template <int NT, bool MIXED, bool NEAR_IN>
 __global__ void __launch_bounds__(NT) pose_kernel(PoseArgs a) {
     const int item = blockIdx.x;
     if (item >= a.items[0]) return;   // uniform over the CTA
@@ -281,7 +258,6 @@ __global__ void __launch_bounds__(NT) pose_kernel(PoseArgs a) {
     double *ed = reinterpret_cast<double *>(st.lob + kStages * kCH);
     float4 *stf = reinterpret_cast<float4 *>(ed + 4 * kCH);
     double *std4 = reinterpret_cast<double *>(stf + a.n_types);
-    float4 *stx = reinterpret_cast<float4 *>(std4 + 4 * a.n_types);   // X2 type table
 
     const int tid = threadIdx.x;
     const int bin = a.items[1 + 3 * item], first = a.items[2 + 3 * item],
@@ -294,7 +270,6 @@ __global__ void __launch_bounds__(NT) pose_kernel(PoseArgs a) {
 #pragma unroll
         for (int k = 0; k < 4; ++k) std4[4 * t + k] = a.td[4 * t + k];
     }
-    if constexpr (X2) far_types_x2<NT>(stx, a.tf, a.n_types);
     if (tid == 0) {
         for (int s = 0; s < kStages; ++s) mbar_init(&st.bar[s], 1);
         fence_mbar_init();
@@ -373,17 +348,8 @@ __global__ void __launch_bounds__(NT) pose_kernel(PoseArgs a) {
             // inner entries first, then the shell (the chunk may straddle them)
             const float4 *hb = st.hib + s * kCH;
             const int split = min(max(r.n_near + r.n_inner - start, 0), len);
-            if constexpr (X2) {
-                float4 *xb = reinterpret_cast<float4 *>(ed);
-                far_expand<NT>(hb, xb, len);
-                __syncthreads();
-                pose_far<false, true>(xb, stx, 0, split, nsx, nsy, nsz, a.rc2f, E, F, shift_sum);
-                pose_far<true, true>(xb, stx, split, len, nsx, nsy, nsz, a.rc2f, E, F,
-                                     shift_sum);
-            } else {
-                pose_far<false>(hb, stf, 0, split, nsx, nsy, nsz, a.rc2f, E, F, shift_sum);
-                pose_far<true>(hb, stf, split, len, nsx, nsy, nsz, a.rc2f, E, F, shift_sum);
-            }
+            pose_far<false>(hb, stf, 0, split, nsx, nsy, nsz, a.rc2f, E, F, shift_sum);
+            pose_far<true>(hb, stf, split, len, nsx, nsy, nsz, a.rc2f, E, F, shift_sum);
         }
         __syncthreads();
         if (tid == 0 && c + kStages < plan.n_chunks)
@@ -497,9 +463,7 @@ int pose_enqueue(System *sys, int n, const double *centers, const double *quats,
         return fail(VEXT_ERR_ARGUMENT, "unknown precision mode %d", o.mode);
     const double r_split = o.mode == VEXT_MODE_FP64 ? 1e30 : o.r_split;
     RegionSet *rs = nullptr;
-    const double width = o.variant & kPoseVariantBin100 ? 1.0
-                         : o.variant & kPoseVariantBin075 ? 0.75 : kBinWidth;
-    VEXT_TRY(get_bin_regions(sys, r_split, &rs, st, width));
+    VEXT_TRY(get_bin_regions(sys, r_split, &rs, st));
     const int n_bins = rs->n_regions;
     // Fewer than 64 poses per bin on average: the binned pipeline would give
     // most of its per-bin CTAs a handful of poses for a whole list each; one
@@ -562,17 +526,14 @@ int pose_enqueue(System *sys, int n, const double *centers, const double *quats,
     VEXT_CUDA(cudaGetLastError());
     pose_scatter_kernel<<<pb, 256, 0, st>>>(a);
     VEXT_CUDA(cudaGetLastError());
-    const size_t smem = kStageBytes + (size_t)kCH * 4 * sizeof(double) + (size_t)a.n_types * 96;
+    const size_t smem = kStageBytes + (size_t)kCH * 4 * sizeof(double) + (size_t)a.n_types * 48;
     double rho = 0;
     for (const RegionInfo &r : rs->h_info) rho = std::max(rho, r.rho);
     const bool near_in = o.mode == VEXT_MODE_MIXED &&
                          r_split + 2.0 * (rho + sys->max_offset) + 1e-6 < sys->cutoff;
-    const bool x2 = o.variant & kPoseVariantX2;
     auto kernel = o.mode != VEXT_MODE_MIXED ? pose_kernel<kPoseThreads, false, false>
-                  : near_in ? (x2 ? pose_kernel<kPoseThreads, true, true, true>
-                                  : pose_kernel<kPoseThreads, true, true>)
-                            : (x2 ? pose_kernel<kPoseThreads, true, false, true>
-                                  : pose_kernel<kPoseThreads, true, false>);
+                  : near_in                 ? pose_kernel<kPoseThreads, true, true>
+                                            : pose_kernel<kPoseThreads, true, false>;
     VEXT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kernel<<<max_items, kPoseThreads, smem, st>>>(a);
     VEXT_CUDA(cudaGetLastError());

@@ -10,7 +10,9 @@ and then, on a machine with a CUDA GPU,
     python tests/golden/make_string_golden.py run --out <dir>
 
 writes each case's ``input.dat`` (the native input layout) and ``--initial``
-path, runs the solver with ``Running_steps`` = 1, 5 and 200, and keeps its
+path, runs the solver with ``Running_steps`` = 1, 2, 5, 6, 100, 101, 199 and
+200 (each run from the same initial path, so consecutive counts give single
+iterations at several points of the run), and keeps its
 path files (``<out>.initial`` / ``<out>.final``: seven ``%.17g`` columns a b c
 alpha beta gamma E, RC_main.cu:2555-2585) and its stdout summary lines
 (``info:``, ``legacy_selection:``, ``final_convergence:``, ``path_review:``).
@@ -45,7 +47,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
 SOLVER = REPO / "oracle" / "_ref" / "string_triclinic_cuda"
-STEPS = (1, 5, 200)
+STEPS = (1, 2, 5, 6, 100, 101, 199, 200)
 DELTA_FRAC = 1e-4
 DELTA_ANGLE_DEG = 1.0
 MARKERS = ("info:", "legacy_selection:", "final_convergence:", "path_review:")
