@@ -103,3 +103,36 @@ def test_string_run_200_iterations_and_files(tmp_path):
     init = tmp_path / "initial.dat"
     init.write_text("\n".join("\t".join(f"{v:.17g}" for v in row) for row in path) + "\n")
     np.testing.assert_array_equal(read_initial(init, 64), path)
+
+
+@pytest.mark.parametrize("name", ["c4", "skew"])
+def test_reference_difference_mode_reproduces_reference_solver(golden, name):
+    """The GPU update with the reference's own one-sided-difference forces
+    (VEXT_STRING_REFERENCE_FD, FP64 energies) against the path files of the
+    reference String solver built from source: 1, 2, 5 and 6 iterations from
+    the initial path, and single iterations from the reference's own path
+    after 1, 5, 100 and 199 iterations; positions to 1e-10, angles to 1e-9 rad
+    (plus, per image, the step-direction uncertainty of forces that are
+    differences of FP64 energies, test_string_reference.step_tolerances);
+    energies of the final paths to 1e-10 relative."""
+    import json
+
+    from test_string_reference import assert_path_close, load_case, step_tolerances
+    g = golden("string_reference.npz")
+    m = json.loads(str(g["meta"]))[name]
+    case = load_case(g, name)
+    hf, ha = m["delta_frac"], m["delta_angle_deg"] * np.pi / 180
+    start = g[f"{name}_start"]
+    runs = [(start, k, f"{name}_final_{k}") for k in m["steps"] if k <= 6]
+    runs += [(g[f"{name}_final_{k}"][:, :6], 1, f"{name}_final_{k + 1}")
+             for k in (1, 5, 100, 199)]
+    with VextSystem(case) as system:
+        for path0, steps, key in runs:
+            path, energy, res = run_string(
+                system, path0, mode=FP64, direction=m["direction"], max_iterations=steps,
+                delta_frac=hf, delta_angle_rad=ha, gradient=_lib.VEXT_STRING_REFERENCE_FD)
+            assert res["iterations"] == steps
+            tol_pos, tol_ang = step_tolerances(case, path0, hf, ha, steps)
+            assert_path_close(path, g[key], tol_pos, tol_ang, key)
+            np.testing.assert_allclose(energy, string_oracle.pose_energy(case, path),
+                                       rtol=1e-10, atol=1e-8)
