@@ -755,7 +755,7 @@ def bench_batch(args, size, axes, device, stream, adjoint=False):
     return result
 
 
-def run_profile_case(kind):
+def run_profile_case(kind, batch_shape=0):
     """Short, fixed cases for ncu (no timing is reported from them)."""
     import torch
     from string_vext_b200 import synth
@@ -772,7 +772,7 @@ def run_profile_case(kind):
             e = torch.empty((64, 60, 60, 60), dtype=torch.float32, device="cuda")
             g = torch.empty((64, 60, 60, 60, 6), dtype=torch.float32, device="cuda")
             for _ in range(2):
-                system.field_adjoint_device(60, axes, e, g)
+                system.field_adjoint_device(60, axes, e, g, batch_shape=batch_shape)
             torch.cuda.synchronize()
         else:
             n = 1 << 20
@@ -806,10 +806,14 @@ def main():
                              "adjoint full_field fields (the first builds, autotunes and "
                              "captures), 'pose' = two 2^20-pose forward+adjoint batches of the "
                              "same framework")
+    parser.add_argument("--batch-shape", type=int, default=0,
+                        help="with --profile adjoint: 1 + the index of the CTA shape to run "
+                             "instead of the autotuner's pick (one launch per call, no tuning "
+                             "launches)")
     args = parser.parse_args()
     ensure_built()
     if args.profile:
-        run_profile_case(args.profile)
+        run_profile_case(args.profile, args.batch_shape)
         return
     rank, world, local_rank = ranks.rank_info()
     if args.impl == "reference":
