@@ -53,7 +53,7 @@ METRIC = "Vext pose evals/s at <=1e-4 K vs FP64, fwd+adjoint evals/s; % FP32 pea
 FAR_DRAM_BYTES_FULL_FIELD = 744_213_504 + 100_719_360
 # the same for one forward + adjoint batch_field_kernel launch on full_field,
 # from an ncu capture (--set full) of `bench.py --profile adjoint`.
-ADJ_DRAM_BYTES_FULL_FIELD = 805_613_568 + 368_731_648
+ADJ_DRAM_BYTES_FULL_FIELD = 770_997_760 + 366_555_904
 CPU_CENTERS_PER_CORE_S = 900.0   # reference driver throughput estimate used to size the sample
 
 
@@ -348,8 +348,9 @@ def run_ours(args, rank, world, local_rank):
     line = {"metric": METRIC, "value": value, "unit": "poses/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32x2+f64 (pairs < 6 A in FP64, beyond in packed FP32 with FP64-flushed "
-                     "partial sums; FP64 energy refinement band)",
+            "dtype": "f32x2+f64 (pairs < 5 A in FP64, beyond in packed FP32 with FP64-flushed "
+                     "partial sums; FP64 energy refinement band; FP64 re-evaluation of poses "
+                     "with a shell pair within 1e-4 A^2 of the cutoff)",
             "data": "synthetic", "config": config_of(args.workload, size),
             "step": "forward + adjoint of every pose: energy, dE/d(center), tangent dE/du; "
                     "region lists resident (built once per framework, reported as setup)",

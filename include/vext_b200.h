@@ -337,6 +337,10 @@ VEXT_API int vext_batch_status(vext_batch batch);
 VEXT_API int vext_batch_destroy(vext_batch batch);
 VEXT_API int vext_batch_info(vext_batch batch, int64_t *work_items, int64_t *poses,
                              int64_t *list_bytes, int *shape, int *grid);
+/* Poses the last replay re-evaluated in FP64 (energies in the refinement
+ * band; for forward + adjoint batches also poses with a shell pair within
+ * 1e-4 A^2 of the cutoff), after waiting for the device. */
+VEXT_API int vext_batch_refined(vext_batch batch, int64_t *poses);
 /* The autotuner's candidates (kernel shape index, resident CTAs, sample time
  * in ms, shape name: threads x directors per thread[/CTAs-per-SM bound]),
  * at most max_candidates of them; any output may be NULL. */

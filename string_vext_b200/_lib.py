@@ -177,6 +177,8 @@ def load(path=None) -> ctypes.CDLL:
     lib.vext_batch_info.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int64)] * 3 + \
         [ctypes.POINTER(ci)] * 2
     lib.vext_batch_info.restype = ci
+    lib.vext_batch_refined.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+    lib.vext_batch_refined.restype = ci
     lib.vext_string_default_params.argtypes = [ctypes.POINTER(StringParams)]
     lib.vext_string_default_params.restype = None
     lib.vext_string_run.argtypes = [vp, ci, vp, vp, ctypes.POINTER(StringParams),

@@ -15,10 +15,12 @@
 // recomputes in FP64.
 //
 // Autotuning: the CTA shape of the mode's table (128 threads x 4 directors
-// or 256 threads x 2, register-resident or shared-memory gradient sums) and
-// the number of resident CTAs per SM are chosen by timing each candidate on
-// a strided 1/16 sample of the queue at creation; the winner is captured
-// into the graph.  The batch
+// or 256 threads x 2, register-resident or shared-memory gradient sums, far
+// entry loop unrolled once or twice) and the number of resident CTAs per SM
+// are chosen by timing each candidate twice on a strided sample of the queue
+// (stride n / (16 x SMs), clamped to 1..64) at creation; the winner is kept
+// per (device, kind, size class) so later batches of that class skip the
+// timing, and is captured into the graph.  The batch
 // keeps pointers to its systems' region lists: the systems must outlive it
 // and not be invalidated while it exists.
 #include <algorithm>
@@ -40,6 +42,7 @@ struct BatchSys {
     double rc2;
     float rc2f;
     double off0, off1;
+    double floor_out2;          // |d0|^2 beyond which no site is inside a contact floor
     int S, O;
     const double *axes;
     const RegionInfo *regs;
@@ -71,11 +74,12 @@ struct BatchArgs {
 // per entry) and shell.
 // GSUM: the FP64 gradient sums wait in shared memory (gsum) during the far
 // passes, so those passes hold only the energy sums and FP32 partials.
-// BORDER: border[p] receives the smallest |q - rc^2| (FP32) of director p
+// BORDER 1: border[p] receives the smallest |q - rc^2| (FP32) of director p
 // over the masked shell pairs, for the FP64 re-evaluation of poses with a
-// pair too close to the cutoff for the FP32 test.
+// pair too close to the cutoff for the FP32 test; 2: the smallest
+// | |d0 . u| - |T*| | (symmetric sites), 2 |o| times which is the former.
 template <int CB, int G, int P, bool NEWTON, bool RCP1, int UNROLL, int FLUSH, bool GSUM,
-          bool BORDER>
+          int BORDER>
 __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSys &y,
                                                const RegionInfo &r, Stager &st, double *ed,
                                                const float4 *stf, const double *std4,
@@ -87,62 +91,30 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
     adj_zero(acc);
 #pragma unroll
     for (int p = 0; p < P; ++p) border[p] = __int_as_float(0x7f800000);   // +inf
-    if constexpr (GSUM) {
-        static_assert(PP <= 2, "two director pairs at most");
-        // near pairs two directors at a time (the near list is staged once
-        // per pair): the FP64 sums of two directors in registers, their
-        // gradient parts parked in gsum, the energies kept in acc
-        const NearGeom g = near_geom(cx, cy, cz, y.off0, y.off1, y.rc2);
+    double shift_sum = 0.0;   // inner and near entries: every pair inside the cutoff
+    // near pairs (FP64): with GSUM two directors at a time (the near list is
+    // staged once per pair; their gradient sums then wait in gsum during the
+    // far passes and only the energies stay in registers), else all P in one
+    // pass
+    constexpr int NP = GSUM ? 2 : P;
+    static_assert(P % NP == 0 && (!GSUM || PP <= 2), "director split");
 #pragma unroll 1
-        for (int half = 0; half < PP; ++half) {
-            AdjAcc a2[2];
-            adj_zero(a2);
-            double ux[2], uy[2], uz[2];
+    for (int half = 0; half < P / NP; ++half) {
+        AdjAcc a2[NP];
+        adj_zero(a2);
+        double ux[NP], uy[NP], uz[NP];
 #pragma unroll
-            for (int p = 0; p < 2; ++p) {
-                const int o = min(obase + G * (2 * half + p), y.O - 1);
-                ux[p] = y.axes[3 * o];
-                uy[p] = y.axes[3 * o + 1];
-                uz[p] = y.axes[3 * o + 2];
-            }
-            ChunkPlan plan;
-            plan.init_range(r.off, r.n_near, r.n_near);
-            stage_prologue(st, plan, y.hi, y.lo, seq);
-            for (int c = 0; c < plan.n_chunks; ++c) {
-                if (!stage_wait(st, plan, c, seq, a.status)) return false;
-                int start, len;
-                bool near;
-                plan.chunk(c, start, len, near);
-                const int s = (seq + c) % kStages;
-                near_convert<NT>(st.hib + s * kCH, st.lob + s * kCH, ed, len);
-                __syncthreads();
-                if (y.near_mode == 2) near_chunk_adj<2, 2>(ed, std4, len, g, ux, uy, uz, a2);
-                else near_chunk_adj<2, 1>(ed, std4, len, g, ux, uy, uz, a2);
-                stage_next(st, plan, y.hi, y.lo, c, seq);
-            }
-            seq += plan.n_chunks;
-            grad_store<NT>(gsum, a2, 2 * half);
-            if (half == 0) {
-                acc[0].e = a2[0].e;
-                acc[1].e = a2[1].e;
-            } else {
-                acc[2 * PP - 2].e = a2[0].e;
-                acc[2 * PP - 1].e = a2[1].e;
-            }
-        }
-    } else {
-        double ux[P], uy[P], uz[P];
-#pragma unroll
-        for (int p = 0; p < P; ++p) {
-            const int o = min(obase + G * p, y.O - 1);
+        for (int p = 0; p < NP; ++p) {
+            const int o = min(obase + G * (NP * half + p), y.O - 1);
             ux[p] = y.axes[3 * o];
             uy[p] = y.axes[3 * o + 1];
             uz[p] = y.axes[3 * o + 2];
         }
-        const NearGeom g = near_geom(cx, cy, cz, y.off0, y.off1, y.rc2);
+        const NearGeom g = near_geom(cx, cy, cz, y.off0, y.off1, y.rc2, y.floor_out2);
         ChunkPlan plan;
         plan.init_range(r.off, r.n_near, r.n_near);
         stage_prologue(st, plan, y.hi, y.lo, seq);
+        double sh_half = 0.0;
         for (int c = 0; c < plan.n_chunks; ++c) {
             if (!stage_wait(st, plan, c, seq, a.status)) return false;
             int start, len;
@@ -151,13 +123,26 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
             const int s = (seq + c) % kStages;
             near_convert<NT>(st.hib + s * kCH, st.lob + s * kCH, ed, len);
             __syncthreads();
-            if (y.near_mode == 2) near_chunk_adj<P, 2>(ed, std4, len, g, ux, uy, uz, acc);
-            else near_chunk_adj<P, 1>(ed, std4, len, g, ux, uy, uz, acc);
+            if (y.near_mode == 2) near_chunk_adj<NP, 2>(ed, std4, len, g, ux, uy, uz, a2, sh_half);
+            else near_chunk_adj<NP, 1>(ed, std4, len, g, ux, uy, uz, a2, sh_half);
             stage_next(st, plan, y.hi, y.lo, c, seq);
         }
         seq += plan.n_chunks;
+        if (half == 0) shift_sum = sh_half;   // the same entries in every pass
+        // acc indices stay compile-time constants (a runtime index would put
+        // acc in local memory)
+        if constexpr (GSUM) {
+            grad_store<NT>(gsum, a2, NP * half);
+#pragma unroll
+            for (int h = 0; h < P / NP; ++h)
+                if (h == half)
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) acc[NP * h + p].e = a2[p].e;
+        } else {
+#pragma unroll
+            for (int p = 0; p < NP; ++p) acc[p] = a2[p];
+        }
     }
-    double shift_sum = 0.0;
     {
         float2 ux[PP], uy[PP], uz[PP];
 #pragma unroll
@@ -210,8 +195,10 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
 // FP32 gradient partials flushed every 16 / 64 entries instead of once per
 // 128-entry chunk; 8 = as 1 with the FP64 gradient sums in shared memory
 // during the far passes (fewer registers: more resident CTAs); 11 / 12 = as
-// 8 / 1 with the far entry loop unrolled twice.
-template <int CB, int G, int P, int MINB, int ADJ, bool BORDER = false>
+// 8 / 1 with the far entry loop unrolled twice.  BORDER: 0 none, 1 the
+// cutoff-border test per site (|q - rc^2|), 2 per director (| |d0 . u| -
+// |T*| |, symmetric sites only).
+template <int CB, int G, int P, int MINB, int ADJ, int BORDER = 0>
 __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
     constexpr int NT = CB * G, PP = P / 2;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -224,6 +211,7 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
     float4 *stf = reinterpret_cast<float4 *>(ed + 4 * kCH);
     const int tid = threadIdx.x;
     constexpr bool kGsum = ADJ == 8 || ADJ == 11;
+    constexpr int kUnroll = ADJ == 5 || ADJ == 11 || ADJ == 12 ? 2 : 1;
     init_barriers(st);
     int last_sys = -1;
     unsigned seq = 0;
@@ -255,11 +243,9 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
         float border[ADJ ? P : 1];
         if constexpr (ADJ) {
             double *gsum = reinterpret_cast<double *>(std4 + 4 * y.n_types);
-            if (!batch_item_adj<CB, G, P, ADJ == 2, ADJ == 1 || ADJ >= 5,
-                                ADJ == 5 || ADJ >= 11 ? 2 : 1,
-                                ADJ == 6 ? 16 : ADJ == 7 ? 64 : 128,
-                                kGsum, BORDER>(a, y, r, st, ed, stf, std4, gsum, seq, cx, cy,
-                                               cz, obase, e, gr, border))
+            if (!batch_item_adj<CB, G, P, ADJ == 2, ADJ == 1 || ADJ >= 5, kUnroll,
+                                ADJ == 6 ? 16 : ADJ == 7 ? 64 : 128, kGsum, BORDER>(
+                    a, y, r, st, ed, stf, std4, gsum, seq, cx, cy, cz, obase, e, gr, border))
                 return;
         } else {
         // ---- near pairs (FP64)
@@ -351,7 +337,13 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
                             gd[2] = make_float2((float)gp[4], (float)gp[5]);
                         }
                         bool refine = v > a.band_lo && v < a.band_hi;
-                        if constexpr (ADJ && BORDER) refine |= border[2 * j + h] < kBorderTol;
+                        if constexpr (ADJ && BORDER) {
+                            // |q - rc^2|; the director-space distance scaled by 2 |o|
+                            const float bq = BORDER == 2
+                                                 ? border[2 * j + h] * (float)(2.0 * fabs(y.off0))
+                                                 : border[2 * j + h];
+                            refine |= bq < kBorderTol;
+                        }
                         if (refine) {
                             const int k = atomicAdd(&a.refine[0], 1);
                             if (k < a.refine_cap) {
@@ -415,8 +407,8 @@ __global__ void batch_refine_kernel(BatchArgs a) {
 // FP64 re-evaluation of the flagged poses of a forward + adjoint batch (the
 // refinement band, and poses with a shell pair within kBorderTol of the
 // cutoff): energy and gradient, one warp per pose, the pair test and terms of
-// plain_fp64_adj_kernel (fp64_pose_pairs) with the lanes striding over the
-// region's list.
+// plain_fp64_adj_kernel (fp64_pose_pairs_both) with the lanes striding over
+// the region's list.
 __global__ void batch_refine_adj_kernel(BatchArgs a) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -436,8 +428,8 @@ __global__ void batch_refine_adj_kernel(BatchArgs a) {
                      (gk + .5) / y.S - r.of[2], cx, cy, cz);
         const double u[3] = {y.axes[3 * o], y.axes[3 * o + 1], y.axes[3 * o + 2]};
         double e = 0.0, g[6];
-        fp64_pose_pairs(y.hi, y.lo, y.td, r.off, r.n_total, lane, 32, y.rc2, y.off0, y.off1, cx,
-                        cy, cz, u, e, g);
+        fp64_pose_pairs_both(y.hi, y.lo, y.td, r.off, r.n_total, lane, 32, y.rc2, y.off0,
+                             y.off1, cx, cy, cz, u, e, g);
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
             e += __shfl_xor_sync(0xffffffffu, e, off);
@@ -501,12 +493,18 @@ static const BatchKernel kAdjointFlush64Kernels[] = {   // accuracy/speed study
 static const BatchKernel kForwardCb8Kernels[] = {
     {batch_field_kernel<8, 16, 4, 4, 0>, 128, "8c 128x4"},
     {batch_field_kernel<8, 32, 2, 3, 0>, 256, "8c 256x2"}};
-static const BatchKernel kAdjointCb8Kernels[] = {
-    {batch_field_kernel<8, 16, 4, 3, 8, true>, 128, "8c 128x4/3 gsum"},
-    {batch_field_kernel<8, 16, 4, 2, 1, true>, 128, "8c 128x4"},
-    {batch_field_kernel<8, 32, 2, 2, 1, true>, 256, "8c 256x2"},
-    {batch_field_kernel<8, 16, 4, 3, 11, true>, 128, "8c 128x4/3 gsum unroll2"},
-    {batch_field_kernel<8, 16, 4, 2, 12, true>, 128, "8c 128x4 unroll2"}};
+static const BatchKernel kAdjointCb8Kernels[] = {   // symmetric sites: border per director
+    {batch_field_kernel<8, 16, 4, 3, 8, 2>, 128, "8c 128x4/3 gsum"},
+    {batch_field_kernel<8, 16, 4, 2, 1, 2>, 128, "8c 128x4"},
+    {batch_field_kernel<8, 32, 2, 2, 1, 2>, 256, "8c 256x2"},
+    {batch_field_kernel<8, 16, 4, 3, 11, 2>, 128, "8c 128x4/3 gsum unroll2"},
+    {batch_field_kernel<8, 16, 4, 2, 12, 2>, 128, "8c 128x4 unroll2"}};
+static const BatchKernel kAdjointCb8SiteBorderKernels[] = {   // any sites: border per site
+    {batch_field_kernel<8, 16, 4, 3, 8, 1>, 128, "8c 128x4/3 gsum, border/site"},
+    {batch_field_kernel<8, 16, 4, 2, 1, 1>, 128, "8c 128x4, border/site"},
+    {batch_field_kernel<8, 32, 2, 2, 1, 1>, 256, "8c 256x2, border/site"},
+    {batch_field_kernel<8, 16, 4, 3, 11, 1>, 128, "8c 128x4/3 gsum unroll2, border/site"},
+    {batch_field_kernel<8, 16, 4, 2, 12, 1>, 128, "8c 128x4 unroll2, border/site"}};
 // the same without the cutoff-border test (timing study: its cost)
 static const BatchKernel kAdjointCb8NoBorderKernels[] = {
     {batch_field_kernel<8, 16, 4, 3, 8>, 128, "8c 128x4/3 gsum, no border test"},
@@ -521,7 +519,8 @@ constexpr int kMaxCandidates = 12;
 // 4 / 5 default with FP32 gradient partials over 16 / 64 entries (a whole
 // 128-entry chunk by default; the energy partials always cover 16), 6 default
 // on 8-center regions with 64-director items, 7 forward on 8-center regions,
-// 8 as 6 without the cutoff-border test
+// 8 as 6 without the cutoff-border test, 9 as 6 with the border test per site
+// (guests whose sites are not symmetric about the center)
 static int batch_kernel_count(int kind) {
     switch (kind) {
     case 0: return VEXT_COUNT(kForwardKernels);
@@ -532,6 +531,7 @@ static int batch_kernel_count(int kind) {
     case 6: return VEXT_COUNT(kAdjointCb8Kernels);
     case 7: return VEXT_COUNT(kForwardCb8Kernels);
     case 8: return VEXT_COUNT(kAdjointCb8NoBorderKernels);
+    case 9: return VEXT_COUNT(kAdjointCb8SiteBorderKernels);
     default: return VEXT_COUNT(kAdjointRcp3Kernels);
     }
 }
@@ -546,6 +546,7 @@ static const BatchKernel &batch_kernel(int kind, int shape) {
     case 6: return kAdjointCb8Kernels[shape];
     case 7: return kForwardCb8Kernels[shape];
     case 8: return kAdjointCb8NoBorderKernels[shape];
+    case 9: return kAdjointCb8SiteBorderKernels[shape];
     default: return kAdjointRcp3Kernels[shape];
     }
 }
@@ -567,7 +568,7 @@ static int batch_kind(const Options &o, bool adj) {
 
 int batch_item_directors(const Options &o, bool adj) {
     const int kind = batch_kind(o, adj);
-    return kind == 6 || kind == 7 || kind == 8 ? 64 : 32;
+    return kind >= 6 && kind <= 9 ? 64 : 32;
 }
 
 }  // namespace vext
@@ -699,7 +700,7 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
     VEXT_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     VEXT_CUDA(cudaMalloc(&b->d_axes, sizeof(double) * 3 * n_axes));
     VEXT_CUDA(cudaMemcpy(b->d_axes, axes, sizeof(double) * 3 * n_axes, cudaMemcpyHostToDevice));
-    // regions of 16 centers x items of 32 directors, or 8 x 64 (kinds 6, 7)
+    // regions of 16 centers x items of 32 directors, or 8 x 64 (kinds 6-9)
     const int kOB = batch_item_directors(b->opt, b->adj), cb = 512 / kOB;
     std::vector<BatchSys> hs(n_systems);
     std::vector<std::pair<long long, int4>> items;
@@ -748,6 +749,16 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
         y.rc2f = (float)y.rc2;
         y.off0 = sys->offsets[0];
         y.off1 = sys->offsets[1];
+        {
+            // a site lies at least |d0| - max|o| from the entry: beyond
+            // (sqrt(max floor2) + max|o|), with a relative margin far above
+            // FP64 rounding, no pair of the pose is inside a floor
+            double fl = 0.0;
+            for (int t = 0; t < sys->n_types; ++t) fl = std::max(fl, sys->h_td[4 * t + 3]);
+            const double rf = (std::sqrt(fl) + std::max(std::fabs(y.off0), std::fabs(y.off1))) *
+                                  (1.0 + 1e-9) + 1e-9;
+            y.floor_out2 = rf * rf;
+        }
         y.S = size;
         y.O = n_axes;
         y.axes = b->d_axes;
@@ -801,6 +812,12 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
     const int size_class =
         (int)std::lround(std::log2(std::max(mean_len, 1.0))) * 64 +
         (int)std::lround(std::log2((double)std::max<size_t>(items.size(), 1)));
+    // the per-director border test of kind 6 assumes symmetric sites (o_1 =
+    // -o_0 != 0); other guests take the same shapes with the per-site test
+    if (b->kind == 6)
+        for (const BatchSys &y : hs)
+            if (y.off0 == 0.0 || std::fabs(y.off0 + y.off1) > 1e-9 * std::fabs(y.off0 - y.off1))
+                b->kind = 9;
     for (const BatchSys &y : hs) b->targets.push_back({y.out, y.grad});
     VEXT_CUDA(cudaMalloc(&b->d_sys, sizeof(BatchSys) * n_systems));
     VEXT_CUDA(cudaMemcpy(b->d_sys, hs.data(), sizeof(BatchSys) * n_systems, cudaMemcpyHostToDevice));
@@ -820,7 +837,6 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
     // candidates: every kernel of the mode at its full occupancy, and at half
     // of it where that still leaves two or more CTAs per SM
     BatchConfig cands[kMaxCandidates];
-    int occ_of[kMaxCandidates] = {};
     int n_cands = 0;
     const int n_kernels = batch_kernel_count(b->kind);
     if (b->opt.batch_shape < 0 || b->opt.batch_shape > n_kernels)
@@ -834,14 +850,9 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
         int occ = 0;
         VEXT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bk.fn, bk.threads, smem));
         if (occ < 1) continue;
-        if (n_cands < kMaxCandidates) {
-            occ_of[n_cands] = occ;
-            cands[n_cands++] = {k, sms * occ};
-        }
-        if (occ >= 4 && n_cands < kMaxCandidates && !b->opt.batch_shape) {
-            occ_of[n_cands] = occ / 2;
+        if (n_cands < kMaxCandidates) cands[n_cands++] = {k, sms * occ};
+        if (occ >= 4 && n_cands < kMaxCandidates && !b->opt.batch_shape)
             cands[n_cands++] = {k, sms * (occ / 2)};
-        }
     }
     if (n_cands == 0) return fail(VEXT_ERR_CAPACITY, "batch kernel does not fit an SM");
     b->n_cands = n_cands;
@@ -975,6 +986,15 @@ extern "C" int vext_batch_status(vext_batch b) {
     if (h[1] > b->refine_cap)
         return fail(VEXT_ERR_CAPACITY, "%d poses in the refinement band; %d refined", h[1],
                     b->refine_cap);
+    return 0;
+}
+
+extern "C" int vext_batch_refined(vext_batch b, int64_t *poses) {
+    if (!b || !poses) return fail(VEXT_ERR_ARGUMENT, "null batch or output");
+    int h = 0;
+    VEXT_CUDA(cudaDeviceSynchronize());
+    VEXT_CUDA(cudaMemcpy(&h, b->d_refine, sizeof(int), cudaMemcpyDeviceToHost));
+    *poses = std::min(h, b->refine_cap);
     return 0;
 }
 

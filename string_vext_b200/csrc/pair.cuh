@@ -99,10 +99,12 @@ struct NearGeom {
     double off0, off1;        // site offsets
     double m0, m1, oo0, oo1;  // -2 o_s and o_s^2
     double rc2;
+    double floor_out2;        // |d0|^2 above which no site is inside a contact floor
 };
 
 __device__ __forceinline__ NearGeom near_geom(double cx, double cy, double cz, double off0,
-                                              double off1, double rc2) {
+                                              double off1, double rc2,
+                                              double floor_out2 = 1e300) {
     NearGeom g;
     g.cx = cx;
     g.cy = cy;
@@ -114,6 +116,7 @@ __device__ __forceinline__ NearGeom near_geom(double cx, double cy, double cz, d
     g.oo0 = off0 * off0;
     g.oo1 = off1 * off1;
     g.rc2 = rc2;
+    g.floor_out2 = floor_out2;
     return g;
 }
 
@@ -223,6 +226,55 @@ __device__ __forceinline__ void fp64_pose_pairs(const float4 *hi, const float4 *
     }
 }
 
+// fp64_pose_pairs for the re-evaluation of flagged poses: the same pair
+// test (d2 from the same hi + lo sums and fma order, d2 >= rc^2 out, the
+// contact floor) and terms, both sites per entry (each entry read once), and
+// the reciprocal of d2 from the hardware seed and two Newton steps instead of
+// a division (within an ulp or two of it).
+__device__ __forceinline__ void fp64_pose_pairs_both(const float4 *hi, const float4 *lo,
+                                                     const double *td, long long off, int n,
+                                                     int first, int step, double rc2,
+                                                     double off0, double off1, double cx,
+                                                     double cy, double cz, const double (&u)[3],
+                                                     double &e, double (&g)[6]) {
+    const double p0x = cx + off0 * u[0], p0y = cy + off0 * u[1], p0z = cz + off0 * u[2];
+    const double p1x = cx + off1 * u[0], p1y = cy + off1 * u[1], p1z = cz + off1 * u[2];
+    double gs[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    for (int k = first; k < n; k += step) {
+        const float4 h = hi[off + k], l = lo[off + k];
+        const double ax = (double)h.x + (double)l.x, ay = (double)h.y + (double)l.y,
+                     az = (double)h.z + (double)l.z;
+        const int t = __float_as_int(h.w);
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const double dx = (s ? p1x : p0x) - ax, dy = (s ? p1y : p0y) - ay,
+                         dz = (s ? p1z : p0z) - az;
+            const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
+            if (d2 >= rc2) continue;
+            const double c12 = td[4 * t], c6 = td[4 * t + 1], fl = td[4 * t + 3];
+            const double s2 = d2 < fl ? fl : d2;
+            const double i2 = rcp64_nr<2>(s2);
+            const double i6 = i2 * i2 * i2;
+            e += c12 * i6 * i6 - c6 * i6 + td[4 * t + 2];
+            if (d2 >= fl) {
+                const double de = 2.0 * (-6.0 * c12 * i6 * i6 + 3.0 * c6 * i6) * i2;
+                gs[s][0] += de * dx;
+                gs[s][1] += de * dy;
+                gs[s][2] += de * dz;
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) g[k] = 0.0;
+#pragma unroll
+    for (int s = 0; s < 2; ++s)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            g[k] += gs[s][k];
+            g[3 + k] += (s ? off1 : off0) * gs[s][k];
+        }
+}
+
 // Project dE/du (g[3..5]) on the plane normal to the unit director u.
 __device__ __forceinline__ void fp64_tangent(const double (&u)[3], double (&g)[6]) {
     const double uu = g[3] * u[0] + g[4] * u[1] + g[5] * u[2];
@@ -245,6 +297,9 @@ struct FarGeom {
     float oo0, oo1;            // o_s^2
     float rc2f;
     float out2;                // |d0|^2 beyond which no site of the pose reaches rc
+    // symmetric sites (o_1 = -o_0 = -o): q_s = rc^2 where s (d0 . u) = T* =
+    // (|d0|^2 + o^2 - rc^2) / (2 o) = |d0|^2 inv2o + tb
+    float inv2o, tb;
 };
 
 __device__ __forceinline__ FarGeom far_geom(double cxd, double cyd, double czd, double off0,
@@ -262,6 +317,9 @@ __device__ __forceinline__ FarGeom far_geom(double cxd, double cyd, double czd, 
     // entry, so beyond this every pair is out by far more than FP32 rounding
     const double rmax = sqrt((double)rc2f) + fmax(fabs(off0), fabs(off1)) + 1e-3;
     g.out2 = (float)(rmax * rmax);
+    const double inv2o = off0 != 0.0 ? 1.0 / (2.0 * off0) : 0.0;
+    g.inv2o = (float)inv2o;
+    g.tb = (float)((off0 * off0 - (double)rc2f) * inv2o);
     return g;
 }
 
@@ -440,13 +498,56 @@ __device__ __forceinline__ void adj_finish(const AdjAcc &a, double off0, double 
     e = a.e;
 }
 
+// The pairs of one near entry (d0 = entry - center, dd = |d0|^2) with the
+// thread's P directors, forward + adjoint.  FLOOR: some site may lie inside
+// the entry type's contact floor (d2 < floor2: energy at the floor, no
+// force); without it the floor tests are left out (the caller checks dd
+// against NearGeom::floor_out2 so that every site is clear of every floor).
+template <int P, int MODE, bool FLOOR>
+__device__ __forceinline__ void near_entry_adj(double dx, double dy, double dz, double dd,
+                                               double2 cc, double2 sh, const NearGeom &g,
+                                               const double (&ux)[P], const double (&uy)[P],
+                                               const double (&uz)[P], AdjAcc (&acc)[P]) {
+    const double m2c12 = -2.0 * cc.x;
+    const double k0 = dd + g.oo0, k1 = dd + g.oo1;
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        const double tt = fma(dx, ux[p], fma(dy, uy[p], dz * uz[p]));
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const double d2 = fma(q ? g.m1 : g.m0, tt, q ? k1 : k0);
+            const double s2 = FLOOR ? fmax(d2, sh.y) : d2;
+            const double i2 = rcp64_nr<1>(s2);
+            const double i6 = i2 * i2 * i2;
+            double fp = (i6 * i2) * fma(m2c12, i6, cc.y);
+            if (FLOOR) fp = d2 < sh.y ? 0.0 : fp;
+            if (MODE == 1) {
+                const bool in = d2 < g.rc2;
+                acc[p].e += in ? fma(i6, fma(cc.x, i6, -cc.y), sh.x) : 0.0;
+                fp = in ? fp : 0.0;
+            } else {
+                acc[p].e = fma(i6, fma(cc.x, i6, -cc.y), acc[p].e);   // shift: per entry
+            }
+            acc[p].h[q][0] = fma(fp, dx, acc[p].h[q][0]);
+            acc[p].h[q][1] = fma(fp, dy, acc[p].h[q][1]);
+            acc[p].h[q][2] = fma(fp, dz, acc[p].h[q][2]);
+            acc[p].f[q] += fp;
+        }
+    }
+}
+
 // FP64 near chunk, forward + adjoint (MODE 1: cutoff test, MODE 2: none);
-// same centre-based q as near_chunk.
+// same centre-based q as near_chunk.  MODE 2 (every pair inside the cutoff):
+// the shift, the same for every pose, is summed once per entry into
+// shift_sum (the caller adds 2 x shift_sum, both sites, to every energy).
+// Entries farther than NearGeom::floor_out2 from the center take the pair
+// loop without the contact-floor tests (nearly all of them; the branch is
+// uniform across the warp but for entries right at that radius).
 template <int P, int MODE>
 __device__ __forceinline__ void near_chunk_adj(const double *ed, const double *std4, int len,
                                                const NearGeom &g, const double (&ux)[P],
                                                const double (&uy)[P], const double (&uz)[P],
-                                               AdjAcc (&acc)[P]) {
+                                               AdjAcc (&acc)[P], double &shift_sum) {
     static_assert(MODE == 1 || MODE == 2, "mixed modes only");
     const double2 *ed2 = reinterpret_cast<const double2 *>(ed);
     const double2 *td2 = reinterpret_cast<const double2 *>(std4);
@@ -455,33 +556,13 @@ __device__ __forceinline__ void near_chunk_adj(const double *ed, const double *s
         const double2 xy = ed2[2 * e], zt = ed2[2 * e + 1];
         const int t = (int)zt.y;
         const double2 cc = td2[2 * t], sh = td2[2 * t + 1];   // (c12, c6), (shift, floor2)
-        const double m2c12 = -2.0 * cc.x;
         const double dx = xy.x - g.cx, dy = xy.y - g.cy, dz = zt.x - g.cz;
         const double dd = fma(dx, dx, fma(dy, dy, dz * dz));
-        const double k0 = dd + g.oo0, k1 = dd + g.oo1;
-#pragma unroll
-        for (int p = 0; p < P; ++p) {
-            const double tt = fma(dx, ux[p], fma(dy, uy[p], dz * uz[p]));
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                const double d2 = fma(q ? g.m1 : g.m0, tt, q ? k1 : k0);
-                const double s2 = fmax(d2, sh.y);
-                const double i2 = rcp64_nr<1>(s2);
-                const double i6 = i2 * i2 * i2;
-                double en = fma(i6, fma(cc.x, i6, -cc.y), sh.x);
-                double fp = d2 < sh.y ? 0.0 : (i6 * i2) * fma(m2c12, i6, cc.y);
-                if (MODE == 1) {
-                    const bool in = d2 < g.rc2;
-                    en = in ? en : 0.0;
-                    fp = in ? fp : 0.0;
-                }
-                acc[p].e += en;
-                acc[p].h[q][0] = fma(fp, dx, acc[p].h[q][0]);
-                acc[p].h[q][1] = fma(fp, dy, acc[p].h[q][1]);
-                acc[p].h[q][2] = fma(fp, dz, acc[p].h[q][2]);
-                acc[p].f[q] += fp;
-            }
-        }
+        if (MODE == 2) shift_sum += sh.x;
+        if (dd > g.floor_out2)
+            near_entry_adj<P, MODE, false>(dx, dy, dz, dd, cc, sh, g, ux, uy, uz, acc);
+        else
+            near_entry_adj<P, MODE, true>(dx, dy, dz, dd, cc, sh, g, ux, uy, uz, acc);
     }
 }
 
@@ -543,7 +624,7 @@ __device__ __forceinline__ void grad_load(double *gsum, AdjAcc (&acc)[P]) {
 // Shell entries beyond every site's cutoff are skipped (they add exactly
 // nothing).
 template <int P, bool NEWTON, int FLUSH, bool MASK, bool RCP1 = true, int UNROLL = 1,
-          int GSUM_NT = 0, bool BORDER = false>
+          int GSUM_NT = 0, int BORDER = 0>
 __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *stf, int len,
                                               const FarGeom &g, const float2 (&ux)[P / 2],
                                               const float2 (&uy)[P / 2],
@@ -576,6 +657,7 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
         for (int e = b0; e < b1; ++e) {
             float2 k0, k1, dx2, dy2, dz2, c12, c6, sh, mc6, m2c12;
             float4 tp;
+            float ts = 0.f;
             {
                 const float4 h = hb[e];
                 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, -)
@@ -593,11 +675,16 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
                 mc6 = make_float2(-tp.y, -tp.y);
                 m2c12 = make_float2(-2.f * tp.x, -2.f * tp.x);
                 if (!MASK) fs += tp.z;
+                if (BORDER == 2) ts = fabsf(fmaf(dd, g.inv2o, g.tb));
             }
 #pragma unroll
             for (int j = 0; j < PP; ++j) {
                 const float2 t =
                     __ffma2_rn(dx2, ux[j], __ffma2_rn(dy2, uy[j], __fmul2_rn(dz2, uz[j])));
+                if (MASK && BORDER == 2) {
+                    border[2 * j] = fminf(border[2 * j], fabsf(fabsf(t.x) - ts));
+                    border[2 * j + 1] = fminf(border[2 * j + 1], fabsf(fabsf(t.y) - ts));
+                }
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
                     const float2 d2 = __ffma2_rn(q ? g.m1 : g.m0, t, q ? k1 : k0);
@@ -616,7 +703,7 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
                                 make_float2(set_lt(d2.x, g.rc2f), set_lt(d2.y, g.rc2f));
                             n3 = __fmul2_rn(n3, m);
                             fe[j] = __ffma2_rn(m, sh, fe[j]);
-                            if (BORDER) {
+                            if (BORDER == 1) {
                                 const float2 x = __fadd2_rn(d2, mrc2);
                                 border[2 * j] = fminf(border[2 * j], fabsf(x.x));
                                 border[2 * j + 1] = fminf(border[2 * j + 1], fabsf(x.y));

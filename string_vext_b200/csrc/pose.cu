@@ -62,7 +62,6 @@ __global__ void pose_prep_kernel(PoseArgs a) {
     a.u[3 * p + 1] = 2.0 * (x * y + w * z);
     a.u[3 * p + 2] = 2.0 * (x * z - w * y);
     const double c0 = a.centers[3 * p], c1 = a.centers[3 * p + 1], c2 = a.centers[3 * p + 2];
-    double f[3];
     int b[3];
     const int nb[3] = {a.nb0, a.nb1, a.nb2};
     bool ok = isfinite(nq) && nq > 0;
@@ -72,7 +71,6 @@ __global__ void pose_prep_kernel(PoseArgs a) {
         ok = ok && isfinite(v);
         v = isfinite(v) ? v - floor(v) : 0.0;
         if (v >= 1.0) v = 0.0;
-        f[k] = v;
         b[k] = min(nb[k] - 1, (int)(v * nb[k]));
         a.wf[3 * p + k] = v;
     }

@@ -241,6 +241,12 @@ class VextBatch:
                 "shape": d.value, "cta_shape": name, "grid": e.value,
                 "adjoint": self.gradients is not None, "tuning": tuning}
 
+    def refined(self) -> int:
+        """Poses the last replay re-evaluated in FP64 (waits for the device)."""
+        n = ctypes.c_int64()
+        _lib.check(self._lib.vext_batch_refined(self.handle, ctypes.byref(n)))
+        return n.value
+
     def tuning(self) -> list:
         """The autotuner's candidates: shape name (threads x directors per
         thread[/CTAs-per-SM bound]), resident CTAs, sample time (ms)."""
