@@ -2,9 +2,10 @@
 // random pose batches, the torch autograd path).
 //
 // Poses are wrapped into the cell (FP64) and binned on a fractional grid of
-// ~1.5 A bins; every bin is a region with its own list (built once per system,
-// system.cu).  One CTA = one work item (a bin and up to kPoseThreads of its
-// poses, one pose per thread).  Pair terms are recomputed, never stored:
+// ~0.75 A bins; every bin is a region with its own list (built once per
+// system, system.cu).  One CTA = one work item (a bin and up to kPoseThreads
+// of its poses, one pose per thread; warps without a pose skip the pair
+// loops).  Pair terms are recomputed, never stored:
 //   E   = sum  c12 i6^2 - c6 i6 + shift                 (d2 < rc^2)
 //   dE/dr_site = sum i2 i6 (6 c6 - 12 c12 i6) (r_site - x)  (floor2 < d2 < rc^2)
 // (inside the contact floor the energy is constant, so its gradient is 0).
@@ -20,7 +21,7 @@
 
 namespace vext {
 
-constexpr int kPoseThreads = 128;
+constexpr int kPoseThreads = 128;   // poses per work item: the CTA width
 
 
 struct PoseArgs {
@@ -39,6 +40,8 @@ struct PoseArgs {
     int *order;              // [n] pose ids sorted by bin
     int *items;              // [0] = count, then (bin, first, len)
     int max_items;
+    int item_poses;          // poses per work item (the CTA width)
+    double floor_out2;       // site-atom d2 above which no type's contact floor applies
     const RegionInfo *regs;
     const float4 *hi, *lo;
     const float4 *tf;
@@ -90,7 +93,7 @@ __global__ void pose_scan_kernel(PoseArgs a) {
     for (int base = 0; base < a.n_bins; base += blockDim.x) {
         const int b = base + threadIdx.x;
         const int cnt = b < a.n_bins ? a.counts[b] : 0;
-        const int nit = (cnt + kPoseThreads - 1) / kPoseThreads;
+        const int nit = (cnt + a.item_poses - 1) / a.item_poses;
         int xc = cnt, xi = nit;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -117,8 +120,8 @@ __global__ void pose_scan_kernel(PoseArgs a) {
                 const int it = pi + k;
                 if (it < a.max_items) {
                     a.items[1 + 3 * it] = b;
-                    a.items[2 + 3 * it] = pc + k * kPoseThreads;
-                    a.items[3 + 3 * it] = min(kPoseThreads, cnt - k * kPoseThreads);
+                    a.items[2 + 3 * it] = pc + k * a.item_poses;
+                    a.items[3 + 3 * it] = min(a.item_poses, cnt - k * a.item_poses);
                 }
             }
         }
@@ -277,6 +280,7 @@ __global__ void __launch_bounds__(NT) pose_kernel(PoseArgs a) {
         for (int c = 0; c < min(kStages, plan.n_chunks); ++c) st.issue(plan, a.hi, a.lo, c, c);
 
     const bool valid = tid < len_p;
+    const bool warp_on = (tid & ~31) < len_p;   // uniform over the warp
     const int p = a.order[first + (valid ? tid : 0)];
     double cx, cy, cz;
     frac_to_cart(a.H, a.wf[3 * p] - r.of[0], a.wf[3 * p + 1] - r.of[1], a.wf[3 * p + 2] - r.of[2],
@@ -318,36 +322,62 @@ __global__ void __launch_bounds__(NT) pose_kernel(PoseArgs a) {
                 ed[4 * e + 3] = (double)__float_as_int(h.w);
             }
             __syncthreads();
-            const double2 *ed2 = reinterpret_cast<const double2 *>(ed);
-            const double2 *td2 = reinterpret_cast<const double2 *>(std4);
+            if (warp_on) {
+                const double2 *ed2 = reinterpret_cast<const double2 *>(ed);
+                const double2 *td2 = reinterpret_cast<const double2 *>(std4);
 #pragma unroll 1
-            for (int e = 0; e < len; ++e) {
-                const double2 xy = ed2[2 * e], zt = ed2[2 * e + 1];
-                const int t = (int)zt.y;
-                const double2 cc = td2[2 * t], sh = td2[2 * t + 1];
-                const double a12 = -12.0 * cc.x, a6 = 6.0 * cc.y;
+                for (int e = 0; e < len; ++e) {
+                    const double2 xy = ed2[2 * e], zt = ed2[2 * e + 1];
+                    const int t = (int)zt.y;
+                    const double2 cc = td2[2 * t], sh = td2[2 * t + 1];
+                    const double a12 = -12.0 * cc.x, a6 = 6.0 * cc.y;
+                    double dx[2], dy[2], dz[2], d2[2];
 #pragma unroll
-                for (int q = 0; q < 2; ++q) {
-                    const double dx = sd[q][0] - xy.x, dy = sd[q][1] - xy.y, dz = sd[q][2] - zt.x;
-                    const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
-                    const double s2 = fmax(d2, sh.y);
-                    const double i2 = MIXED ? rcp64_nr<1>(s2) : __drcp_rn(s2);
-                    const double i6 = i2 * i2 * i2;
-                    const double en = fma(i6, fma(cc.x, i6, -cc.y), sh.x);
-                    const bool in = NEAR_IN || d2 < a.rc2;
-                    const double w = (in && d2 > sh.y) ? i2 * i6 * fma(a12, i6, a6) : 0.0;
-                    E[q] += in ? en : 0.0;
-                    F[q][0] = fma(w, dx, F[q][0]);
-                    F[q][1] = fma(w, dy, F[q][1]);
-                    F[q][2] = fma(w, dz, F[q][2]);
+                    for (int q = 0; q < 2; ++q) {
+                        dx[q] = sd[q][0] - xy.x;
+                        dy[q] = sd[q][1] - xy.y;
+                        dz[q] = sd[q][2] - zt.x;
+                        d2[q] = fma(dx[q], dx[q], fma(dy[q], dy[q], dz[q] * dz[q]));
+                    }
+                    if (MIXED && NEAR_IN && fmin(d2[0], d2[1]) > a.floor_out2) {
+                        // every pair inside the cutoff and clear of the floor:
+                        // no tests, the shift summed once per entry
+                        shift_sum += sh.x;
+#pragma unroll
+                        for (int q = 0; q < 2; ++q) {
+                            const double i2 = rcp64_nr<1>(d2[q]);
+                            const double i6 = i2 * i2 * i2;
+                            E[q] = fma(i6, fma(cc.x, i6, -cc.y), E[q]);
+                            const double w = i2 * i6 * fma(a12, i6, a6);
+                            F[q][0] = fma(w, dx[q], F[q][0]);
+                            F[q][1] = fma(w, dy[q], F[q][1]);
+                            F[q][2] = fma(w, dz[q], F[q][2]);
+                        }
+                        continue;
+                    }
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const double s2 = fmax(d2[q], sh.y);
+                        const double i2 = MIXED ? rcp64_nr<1>(s2) : __drcp_rn(s2);
+                        const double i6 = i2 * i2 * i2;
+                        const double en = fma(i6, fma(cc.x, i6, -cc.y), sh.x);
+                        const bool in = NEAR_IN || d2[q] < a.rc2;
+                        const double w = (in && d2[q] > sh.y) ? i2 * i6 * fma(a12, i6, a6) : 0.0;
+                        E[q] += in ? en : 0.0;
+                        F[q][0] = fma(w, dx[q], F[q][0]);
+                        F[q][1] = fma(w, dy[q], F[q][1]);
+                        F[q][2] = fma(w, dz[q], F[q][2]);
+                    }
                 }
             }
         } else if (MIXED) {
             // inner entries first, then the shell (the chunk may straddle them)
             const float4 *hb = st.hib + s * kCH;
             const int split = min(max(r.n_near + r.n_inner - start, 0), len);
-            pose_far<false>(hb, stf, 0, split, nsx, nsy, nsz, a.rc2f, E, F, shift_sum);
-            pose_far<true>(hb, stf, split, len, nsx, nsy, nsz, a.rc2f, E, F, shift_sum);
+            if (warp_on) {
+                pose_far<false>(hb, stf, 0, split, nsx, nsy, nsz, a.rc2f, E, F, shift_sum);
+                pose_far<true>(hb, stf, split, len, nsx, nsy, nsz, a.rc2f, E, F, shift_sum);
+            }
         }
         __syncthreads();
         if (tid == 0 && c + kStages < plan.n_chunks)
@@ -469,7 +499,8 @@ int pose_enqueue(System *sys, int n, const double *centers, const double *quats,
     if ((long long)n < 64LL * n_bins)
         return pose_warp_enqueue(sys, rs, n, centers, quats, o,
                                  energy ? energy : nullptr, gc, gq, gu, st);
-    const int max_items = n_bins + (n + kPoseThreads - 1) / kPoseThreads;
+    const int item_poses = kPoseThreads;
+    const int max_items = n_bins + (n + item_poses - 1) / item_poses;
     const size_t bytes = pose_scratch_bytes(n, n_bins, max_items, false);
     VEXT_TRY(ensure_capacity(*reinterpret_cast<char **>(&sys->d_pose_scratch),
                              sys->pose_scratch_cap, bytes));
@@ -495,6 +526,15 @@ int pose_enqueue(System *sys, int n, const double *centers, const double *quats,
     a.cursor = bump.take<int>(n_bins);
     a.items = bump.take<int>(1 + 3 * (size_t)max_items);
     a.max_items = max_items;
+    a.item_poses = item_poses;
+    {
+        // beyond sqrt(max floor2) (plus a relative margin far above FP64
+        // rounding) no pair of any type is inside its contact floor
+        double fl = 0.0;
+        for (int t = 0; t < sys->n_types; ++t) fl = std::max(fl, sys->h_td[4 * t + 3]);
+        const double rf = std::sqrt(fl) * (1.0 + 1e-9) + 1e-9;
+        a.floor_out2 = rf * rf;
+    }
     a.regs = rs->d_info;
     a.hi = rs->d_hi;
     a.lo = rs->d_lo;
@@ -533,7 +573,7 @@ int pose_enqueue(System *sys, int n, const double *centers, const double *quats,
                   : near_in                 ? pose_kernel<kPoseThreads, true, true>
                                             : pose_kernel<kPoseThreads, true, false>;
     VEXT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kernel<<<max_items, kPoseThreads, smem, st>>>(a);
+    kernel<<<max_items, item_poses, smem, st>>>(a);
     VEXT_CUDA(cudaGetLastError());
     if (refine) {
         pose_refine_kernel<<<std::min(1184, (n + 7) / 8), 256, 0, st>>>(a);
