@@ -146,7 +146,11 @@ typedef struct {
                                 disables refinement; defaults via
                                 vext_default_options                          */
     int centers_per_region;  /* 16 or 32; 0 = default (16)                    */
-    int variant;             /* pair-kernel shape; 0 = default                */
+    int variant;             /* pair-kernel shape; 0 = default.  Forward +
+                                adjoint batches: bit 4096 re-evaluates poses
+                                with a shell pair within 1.25e-4 A^2 of the
+                                cutoff wholly in FP64 instead of re-testing
+                                only their shell pairs                        */
     int batch_shape;         /* batches: 1 + index of the CTA shape to run at
                                 full occupancy instead of autotuning; 0 =
                                 autotune (vext_batch_tuning lists the shapes);
@@ -339,7 +343,7 @@ VEXT_API int vext_batch_info(vext_batch batch, int64_t *work_items, int64_t *pos
                              int64_t *list_bytes, int *shape, int *grid);
 /* Poses the last replay re-evaluated in FP64 (energies in the refinement
  * band; for forward + adjoint batches also poses with a shell pair within
- * 1e-4 A^2 of the cutoff), after waiting for the device. */
+ * 1.25e-4 A^2 of the cutoff), after waiting for the device. */
 VEXT_API int vext_batch_refined(vext_batch batch, int64_t *poses);
 /* The autotuner's candidates (kernel shape index, resident CTAs, sample time
  * in ms, shape name: threads x directors per thread[/CTAs-per-SM bound]),

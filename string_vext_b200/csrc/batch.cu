@@ -57,6 +57,16 @@ struct BatchSys {
     double *out64;              // FP64 copy of the energies [O][S^3], or null
 };
 
+// Refinement record flag: the pose is outside the refinement band but has a
+// shell pair within kBorderTol of the cutoff; only its shell pairs are
+// re-tested (batch_refine_adj_kernel).
+constexpr int kRepairOnly = 1 << 30;
+
+// vext_options.variant bit: re-evaluate poses with a shell pair near the
+// cutoff in FP64 as a whole instead of repairing their shell pairs (the check
+// of the repair)
+constexpr int kVariantFullRefine = 4096;
+
 struct BatchArgs {
     const BatchSys *sys;
     const int4 *items;          // (system, region, director block, -)
@@ -65,6 +75,7 @@ struct BatchArgs {
     int *refine;                // [0] count, then (system, pose) pairs
     int refine_cap;
     double band_lo, band_hi;
+    int full_refine;            // border poses re-evaluated in FP64 too (kVariantFullRefine)
     int *status;
 };
 
@@ -96,6 +107,9 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
     // staged once per pair; their gradient sums then wait in gsum during the
     // far passes and only the energies stay in registers), else all P in one
     // pass
+    // symmetric sites (kernels with the per-director border test): q_1 = k0 -
+    // m0 t.  All P directors at once with GSUM would spill (slower).
+    constexpr bool SYM = BORDER == 2;
     constexpr int NP = GSUM ? 2 : P;
     static_assert(P % NP == 0 && (!GSUM || PP <= 2), "director split");
 #pragma unroll 1
@@ -123,8 +137,10 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
             const int s = (seq + c) % kStages;
             near_convert<NT>(st.hib + s * kCH, st.lob + s * kCH, ed, len);
             __syncthreads();
-            if (y.near_mode == 2) near_chunk_adj<NP, 2>(ed, std4, len, g, ux, uy, uz, a2, sh_half);
-            else near_chunk_adj<NP, 1>(ed, std4, len, g, ux, uy, uz, a2, sh_half);
+            if (y.near_mode == 2)
+                near_chunk_adj<NP, 2, SYM>(ed, std4, len, g, ux, uy, uz, a2, sh_half);
+            else
+                near_chunk_adj<NP, 1, SYM>(ed, std4, len, g, ux, uy, uz, a2, sh_half);
             stage_next(st, plan, y.hi, y.lo, c, seq);
         }
         seq += plan.n_chunks;
@@ -195,7 +211,8 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
 // FP32 gradient partials flushed every 16 / 64 entries instead of once per
 // 128-entry chunk; 8 = as 1 with the FP64 gradient sums in shared memory
 // during the far passes (fewer registers: more resident CTAs); 11 / 12 = as
-// 8 / 1 with the far entry loop unrolled twice.  BORDER: 0 none, 1 the
+// 8 / 1 with the far entry loop unrolled twice; 17 = as 8 unrolled four
+// times.  BORDER: 0 none, 1 the
 // cutoff-border test per site (|q - rc^2|), 2 per director (| |d0 . u| -
 // |T*| |, symmetric sites only).
 template <int CB, int G, int P, int MINB, int ADJ, int BORDER = 0>
@@ -210,8 +227,8 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
     double *ed = reinterpret_cast<double *>(st.lob + kStages * kCH);   // [kCH][4]
     float4 *stf = reinterpret_cast<float4 *>(ed + 4 * kCH);
     const int tid = threadIdx.x;
-    constexpr bool kGsum = ADJ == 8 || ADJ == 11;
-    constexpr int kUnroll = ADJ == 5 || ADJ == 11 || ADJ == 12 ? 2 : 1;
+    constexpr bool kGsum = ADJ == 8 || ADJ == 11 || ADJ == 17;
+    constexpr int kUnroll = ADJ == 17 ? 4 : ADJ == 5 || ADJ == 11 || ADJ == 12 ? 2 : 1;
     init_barriers(st);
     int last_sys = -1;
     unsigned seq = 0;
@@ -336,18 +353,21 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
                             gd[1] = make_float2((float)gp[2], (float)gp[3]);
                             gd[2] = make_float2((float)gp[4], (float)gp[5]);
                         }
-                        bool refine = v > a.band_lo && v < a.band_hi;
+                        const bool band = v > a.band_lo && v < a.band_hi;
+                        bool near_rc = false;
                         if constexpr (ADJ && BORDER) {
-                            // |q - rc^2|; the director-space distance scaled by 2 |o|
-                            const float bq = BORDER == 2
-                                                 ? border[2 * j + h] * (float)(2.0 * fabs(y.off0))
-                                                 : border[2 * j + h];
-                            refine |= bq < kBorderTol;
+                            // |q - rc^2|, or its director-space estimate scaled by 2 |o|
+                            near_rc = BORDER == 2 ? border[2 * j + h] * (float)(2.0 * fabs(y.off0)) <
+                                                        kBorderTolDir
+                                                  : border[2 * j + h] < kBorderTol;
                         }
-                        if (refine) {
+                        if (band || near_rc) {
+                            // band poses are re-evaluated in FP64, the others
+                            // (kRepairOnly) only have their shell pairs re-tested
                             const int k = atomicAdd(&a.refine[0], 1);
                             if (k < a.refine_cap) {
-                                a.refine[1 + 2 * k] = w.x;
+                                a.refine[1 + 2 * k] =
+                                    w.x | (band || a.full_refine ? 0 : kRepairOnly);
                                 a.refine[2 + 2 * k] = (int)idx;
                             }
                         }
@@ -404,18 +424,27 @@ __global__ void batch_refine_kernel(BatchArgs a) {
     }
 }
 
-// FP64 re-evaluation of the flagged poses of a forward + adjoint batch (the
-// refinement band, and poses with a shell pair within kBorderTol of the
-// cutoff): energy and gradient, one warp per pose, the pair test and terms of
-// plain_fp64_adj_kernel (fp64_pose_pairs_both) with the lanes striding over
-// the region's list.
+// FP64 re-evaluation of the flagged poses of a forward + adjoint batch, one
+// warp per pose, the lanes striding over the region's list:
+// * poses in the refinement band: energy and gradient from every pair in
+//   FP64 (fp64_pose_pairs_both, the pair test and terms of
+//   plain_fp64_adj_kernel);
+// * poses with a shell pair within kBorderTol of the cutoff (kRepairOnly):
+//   each shell pair's inside/outside decision is recomputed with the far
+//   kernel's own FP32 arithmetic (bit for bit: the same operations in the
+//   same order, so the same roundings) and with the FP64 test the oracle
+//   uses (d2 >= rc^2 out); where they differ, the pair's FP64 energy and
+//   gradient terms are added (FP64 inside) or removed (FP64 outside).  Every
+//   other pair of the pose was already decided the same way by both.
 __global__ void batch_refine_adj_kernel(BatchArgs a) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     const int count = min(a.refine[0], a.refine_cap);
     for (int q = warp; q < count; q += nwarps) {
-        const BatchSys &y = a.sys[a.refine[1 + 2 * q]];
+        const int tag = a.refine[1 + 2 * q];
+        const bool repair = (tag & kRepairOnly) != 0;
+        const BatchSys &y = a.sys[tag & ~kRepairOnly];
         const long long idx = a.refine[2 + 2 * q];
         const long long S3 = (long long)y.S * y.S * y.S;
         const int o = (int)(idx / S3);
@@ -428,8 +457,13 @@ __global__ void batch_refine_adj_kernel(BatchArgs a) {
                      (gk + .5) / y.S - r.of[2], cx, cy, cz);
         const double u[3] = {y.axes[3 * o], y.axes[3 * o + 1], y.axes[3 * o + 2]};
         double e = 0.0, g[6];
-        fp64_pose_pairs_both(y.hi, y.lo, y.td, r.off, r.n_total, lane, 32, y.rc2, y.off0,
-                             y.off1, cx, cy, cz, u, e, g);
+        if (repair)
+            shell_border_repair(y.hi, y.lo, y.td, r.off + r.n_near + r.n_inner,
+                                r.n_total - r.n_near - r.n_inner, lane, 32, y.rc2, y.rc2f,
+                                y.off0, y.off1, cx, cy, cz, u, e, g);
+        else
+            fp64_pose_pairs_both(y.hi, y.lo, y.td, r.off, r.n_total, lane, 32, y.rc2, y.off0,
+                                 y.off1, cx, cy, cz, u, e, g);
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
             e += __shfl_xor_sync(0xffffffffu, e, off);
@@ -438,12 +472,23 @@ __global__ void batch_refine_adj_kernel(BatchArgs a) {
         }
         if (lane == 0) {
             fp64_tangent(u, g);
-            y.out[idx] = (float)e;
-            if (y.out64) y.out64[idx] = e;
             float2 *gd = reinterpret_cast<float2 *>(y.grad + 6 * idx);
-            gd[0] = make_float2((float)g[0], (float)g[1]);
-            gd[1] = make_float2((float)g[2], (float)g[3]);
-            gd[2] = make_float2((float)g[4], (float)g[5]);
+            if (repair) {
+                // corrections on top of the far kernel's results
+                const double e64 = (y.out64 ? y.out64[idx] : (double)y.out[idx]) + e;
+                y.out[idx] = (float)e64;
+                if (y.out64) y.out64[idx] = e64;
+                const float2 g0 = gd[0], g1 = gd[1], g2 = gd[2];
+                gd[0] = make_float2((float)((double)g0.x + g[0]), (float)((double)g0.y + g[1]));
+                gd[1] = make_float2((float)((double)g1.x + g[2]), (float)((double)g1.y + g[3]));
+                gd[2] = make_float2((float)((double)g2.x + g[4]), (float)((double)g2.y + g[5]));
+            } else {
+                y.out[idx] = (float)e;
+                if (y.out64) y.out64[idx] = e;
+                gd[0] = make_float2((float)g[0], (float)g[1]);
+                gd[1] = make_float2((float)g[2], (float)g[3]);
+                gd[2] = make_float2((float)g[4], (float)g[5]);
+            }
         }
     }
 }
@@ -498,13 +543,15 @@ static const BatchKernel kAdjointCb8Kernels[] = {   // symmetric sites: border p
     {batch_field_kernel<8, 16, 4, 2, 1, 2>, 128, "8c 128x4"},
     {batch_field_kernel<8, 32, 2, 2, 1, 2>, 256, "8c 256x2"},
     {batch_field_kernel<8, 16, 4, 3, 11, 2>, 128, "8c 128x4/3 gsum unroll2"},
-    {batch_field_kernel<8, 16, 4, 2, 12, 2>, 128, "8c 128x4 unroll2"}};
+    {batch_field_kernel<8, 16, 4, 2, 12, 2>, 128, "8c 128x4 unroll2"},
+    {batch_field_kernel<8, 16, 4, 3, 17, 2>, 128, "8c 128x4/3 gsum unroll4"}};
 static const BatchKernel kAdjointCb8SiteBorderKernels[] = {   // any sites: border per site
     {batch_field_kernel<8, 16, 4, 3, 8, 1>, 128, "8c 128x4/3 gsum, border/site"},
     {batch_field_kernel<8, 16, 4, 2, 1, 1>, 128, "8c 128x4, border/site"},
     {batch_field_kernel<8, 32, 2, 2, 1, 1>, 256, "8c 256x2, border/site"},
     {batch_field_kernel<8, 16, 4, 3, 11, 1>, 128, "8c 128x4/3 gsum unroll2, border/site"},
-    {batch_field_kernel<8, 16, 4, 2, 12, 1>, 128, "8c 128x4 unroll2, border/site"}};
+    {batch_field_kernel<8, 16, 4, 2, 12, 1>, 128, "8c 128x4 unroll2, border/site"},
+    {batch_field_kernel<8, 16, 4, 3, 17, 1>, 128, "8c 128x4/3 gsum unroll4, border/site"}};
 // the same without the cutoff-border test (timing study: its cost)
 static const BatchKernel kAdjointCb8NoBorderKernels[] = {
     {batch_field_kernel<8, 16, 4, 3, 8>, 128, "8c 128x4/3 gsum, no border test"},
@@ -631,6 +678,7 @@ static int batch_launch(vext_batch b, const BatchConfig &cfg, const int4 *items,
     a.refine_cap = b->refine_cap;
     a.band_lo = b->opt.band_lo;
     a.band_hi = b->opt.band_hi;
+    a.full_refine = (b->opt.variant & kVariantFullRefine) != 0;
     a.status = b->d_status;
     const size_t smem = batch_smem(b->max_types, b->adj);
     VEXT_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(int), st));

@@ -128,11 +128,14 @@ struct Mat3 {
     double m[9];  // row-vector cell: cart_j = sum_k frac_k m[3k + j]
 };
 
+// Explicit fused multiply-adds: every kernel that forms a center gets the
+// same roundings (the border repair recomputes the far kernel's FP32
+// decisions bit for bit from the same center).
 __host__ __device__ __forceinline__ void frac_to_cart(const Mat3 &h, double a, double b, double c,
                                                       double &x, double &y, double &z) {
-    x = a * h.m[0] + b * h.m[3] + c * h.m[6];
-    y = a * h.m[1] + b * h.m[4] + c * h.m[7];
-    z = a * h.m[2] + b * h.m[5] + c * h.m[8];
+    x = fma(c, h.m[6], fma(b, h.m[3], a * h.m[0]));
+    y = fma(c, h.m[7], fma(b, h.m[4], a * h.m[1]));
+    z = fma(c, h.m[8], fma(b, h.m[5], a * h.m[2]));
 }
 
 }  // namespace vext

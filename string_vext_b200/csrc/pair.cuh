@@ -281,13 +281,6 @@ __device__ __forceinline__ void fp64_tangent(const double (&u)[3], double (&g)[6
     for (int k = 0; k < 3; ++k) g[3 + k] -= uu * u[k];
 }
 
-// A shell pair whose FP32 q lies within kBorderTol (A^2) of rc^2 may be
-// classified differently by the FP32 test than by the FP64 one.  The FP32 q
-// of a far entry carries at most about 6e-5 A^2 of error at r ~ 13 A (the
-// entry position rounded to FP32 relative to its region origin, 2 |d| x
-// 8.3e-7 A, plus the roundings of |d0|^2, t and the site FMA), so poses with
-// such a pair are re-evaluated in FP64.
-constexpr float kBorderTol = 1e-4f;
 
 // ------------------------------------------------------------ far (FP32x2)
 
@@ -321,6 +314,83 @@ __device__ __forceinline__ FarGeom far_geom(double cxd, double cyd, double czd, 
     g.inv2o = (float)inv2o;
     g.tb = (float)((off0 * off0 - (double)rc2f) * inv2o);
     return g;
+}
+
+// A shell pair is classified by the FP32 test (q < rc^2 in FP32) as by the
+// FP64 one unless its FP32 q lies within kBorderTol (A^2) of rc^2.  Worst
+// case, every error aligned, for |d0| <= 13.4 A: each d0 component off by
+// <= 9.9e-7 A (entry and center rounded to FP32, then the subtraction),
+// which moves |d0|^2 by <= 2 |d0| sqrt(3) 9.9e-7 = 4.6e-5; the roundings of
+// |d0|^2 (3 x 7.6e-6), of t = d0 . u with FP32 u (moving q by <= 5e-6), of
+// |d0|^2 + o^2 and of the site FMA (7.6e-6 each); rc^2 rounded to FP32
+// (7.6e-6): <= 9.8e-5 in all.
+constexpr float kBorderTol = 1.25e-4f;
+// The per-director test estimates min_s |q_s - rc^2| as 2 |o| | |t| - |T*| |
+// from the same FP32 |d0|^2 and t; T* (rounded 1/(2o), offset and FMA) and
+// the missing site roundings put that estimate within 3.6e-5 of the FP32
+// q's own distance, so the director test flags below kBorderTol + 4e-5.
+constexpr float kBorderTolDir = kBorderTol + 4e-5f;
+
+// Border repair of one pose (entries k = first, first + step, ... of the
+// shell range [off, off + n) of its region list): for each site, the far
+// kernel's FP32 inside/outside decision -- recomputed with exactly its
+// operations (far_geom, far_chunk_adj: d0 = hi - c in FP32, |d0|^2 and
+// d0 . u as fused multiply-adds in the same order, q = m t + (|d0|^2 + o^2),
+// inside when q < rc^2 in FP32) -- against the FP64 one (hi + lo positions,
+// d2 >= rc^2 out).  A pair inside in FP64 only adds its FP64 energy (with
+// the shift) and gradient terms to e and g; inside in FP32 only subtracts
+// them.  Entries the far kernel skipped (|d0|^2 beyond FarGeom::out2) are
+// out in both, and so are pairs whose FP32 q lies kBorderTol or more from
+// rc^2 (only the FP32 terms are formed for those).  Shell pairs lie far
+// beyond every contact floor.
+__device__ __forceinline__ void shell_border_repair(const float4 *hi, const float4 *lo,
+                                                    const double *td, long long off, int n,
+                                                    int first, int step, double rc2,
+                                                    float rc2f, double off0, double off1,
+                                                    double cx, double cy, double cz,
+                                                    const double (&u)[3], double &e,
+                                                    double (&g)[6]) {
+    const FarGeom f = far_geom(cx, cy, cz, off0, off1, rc2f);
+    const float ufx = (float)u[0], ufy = (float)u[1], ufz = (float)u[2];
+    e = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) g[k] = 0.0;
+    for (int k = first; k < n; k += step) {
+        const float4 h = hi[off + k];
+        const float dx = h.x - f.cx, dy = h.y - f.cy, dz = h.z - f.cz;
+        const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        if (dd > f.out2) continue;
+        const float t = fmaf(dx, ufx, fmaf(dy, ufy, dz * ufz));
+        const float q0 = fmaf(f.m0.x, t, dd + f.oo0), q1 = fmaf(f.m1.x, t, dd + f.oo1);
+        // beyond kBorderTol of rc^2 the FP32 decision is the FP64 one
+        if (fabsf(q0 - rc2f) >= kBorderTol && fabsf(q1 - rc2f) >= kBorderTol) continue;
+        const float4 l = lo[off + k];
+        const double ax = (double)h.x + (double)l.x, ay = (double)h.y + (double)l.y,
+                     az = (double)h.z + (double)l.z;
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const float q32 = s ? q1 : q0;
+            const double os = s ? off1 : off0;
+            const double px = cx + os * u[0] - ax, py = cy + os * u[1] - ay,
+                         pz = cz + os * u[2] - az;
+            const double d2 = fma(px, px, fma(py, py, pz * pz));
+            const bool in32 = q32 < rc2f, in64 = d2 < rc2;
+            if (in32 == in64) continue;
+            const int ty = __float_as_int(h.w);
+            const double c12 = td[4 * ty], c6 = td[4 * ty + 1];
+            const double i2 = rcp64_nr<2>(d2);
+            const double i6 = i2 * i2 * i2;
+            const double w = in64 ? 1.0 : -1.0;
+            e += w * (c12 * i6 * i6 - c6 * i6 + td[4 * ty + 2]);
+            const double de = w * 2.0 * (-6.0 * c12 * i6 * i6 + 3.0 * c6 * i6) * i2;
+            g[0] += de * px;
+            g[1] += de * py;
+            g[2] += de * pz;
+            g[3] += os * de * px;
+            g[4] += os * de * py;
+            g[5] += os * de * pz;
+        }
+    }
 }
 
 // The earlier forward far chunk, kept for comparison with far_chunk_fwd:
@@ -503,19 +573,20 @@ __device__ __forceinline__ void adj_finish(const AdjAcc &a, double off0, double 
 // the entry type's contact floor (d2 < floor2: energy at the floor, no
 // force); without it the floor tests are left out (the caller checks dd
 // against NearGeom::floor_out2 so that every site is clear of every floor).
-template <int P, int MODE, bool FLOOR>
+template <int P, int MODE, bool FLOOR, bool SYM>
 __device__ __forceinline__ void near_entry_adj(double dx, double dy, double dz, double dd,
                                                double2 cc, double2 sh, const NearGeom &g,
                                                const double (&ux)[P], const double (&uy)[P],
                                                const double (&uz)[P], AdjAcc (&acc)[P]) {
     const double m2c12 = -2.0 * cc.x;
-    const double k0 = dd + g.oo0, k1 = dd + g.oo1;
+    // SYM: o_1 = -o_0, so q_1 = k0 - m0 t
+    const double k0 = dd + g.oo0, k1 = SYM ? k0 : dd + g.oo1;
 #pragma unroll
     for (int p = 0; p < P; ++p) {
         const double tt = fma(dx, ux[p], fma(dy, uy[p], dz * uz[p]));
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-            const double d2 = fma(q ? g.m1 : g.m0, tt, q ? k1 : k0);
+            const double d2 = fma(q ? (SYM ? -g.m0 : g.m1) : g.m0, tt, q ? k1 : k0);
             const double s2 = FLOOR ? fmax(d2, sh.y) : d2;
             const double i2 = rcp64_nr<1>(s2);
             const double i6 = i2 * i2 * i2;
@@ -543,7 +614,7 @@ __device__ __forceinline__ void near_entry_adj(double dx, double dy, double dz, 
 // Entries farther than NearGeom::floor_out2 from the center take the pair
 // loop without the contact-floor tests (nearly all of them; the branch is
 // uniform across the warp but for entries right at that radius).
-template <int P, int MODE>
+template <int P, int MODE, bool SYM = false>
 __device__ __forceinline__ void near_chunk_adj(const double *ed, const double *std4, int len,
                                                const NearGeom &g, const double (&ux)[P],
                                                const double (&uy)[P], const double (&uz)[P],
@@ -560,9 +631,9 @@ __device__ __forceinline__ void near_chunk_adj(const double *ed, const double *s
         const double dd = fma(dx, dx, fma(dy, dy, dz * dz));
         if (MODE == 2) shift_sum += sh.x;
         if (dd > g.floor_out2)
-            near_entry_adj<P, MODE, false>(dx, dy, dz, dd, cc, sh, g, ux, uy, uz, acc);
+            near_entry_adj<P, MODE, false, SYM>(dx, dy, dz, dd, cc, sh, g, ux, uy, uz, acc);
         else
-            near_entry_adj<P, MODE, true>(dx, dy, dz, dd, cc, sh, g, ux, uy, uz, acc);
+            near_entry_adj<P, MODE, true, SYM>(dx, dy, dz, dd, cc, sh, g, ux, uy, uz, acc);
     }
 }
 

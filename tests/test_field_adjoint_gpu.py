@@ -388,3 +388,40 @@ def test_batch_frameworks_gradients_within_bar_for_every_pose():
     for s in systems:
         s.close()
     assert worst < 1e-5, f"worst gradient error {worst}"
+
+
+def test_border_repair_matches_full_fp64_refinement():
+    """Poses with a shell pair within 1.25e-4 A^2 of the cutoff get their shell
+    pairs re-tested (the far kernel's FP32 decision recomputed bit for bit
+    against the FP64 one, misjudged pairs swapped in or out in FP64).  The
+    same batch with those poses wholly re-evaluated in FP64 (variant 4096)
+    flags the same poses, and both results agree within FP32 resolution:
+    energy at float32 storage, gradient 1e-6 relative.  Without the border
+    test (variant 1024) only refinement-band poses are flagged."""
+    cases = synth.batch_frameworks(4)
+    size = 12
+    _, axes = regular_pose_grid(size, 64)
+    axes = normalized_directors(axes)
+    systems = [VextSystem(c) for c in cases]
+    shape = (64, size, size, size)
+    results = {}
+    for label, variant in (("repair", 0), ("full", 4096), ("none", 1024)):
+        outs = [torch.empty(shape, dtype=torch.float32, device="cuda") for _ in systems]
+        grads = [torch.empty(shape + (6,), dtype=torch.float32, device="cuda") for _ in systems]
+        batch = VextBatch(systems, size, axes, outs, gradients=grads, variant=variant)
+        batch.run()
+        batch.check()
+        refined = batch.refined()
+        batch.close()
+        results[label] = (refined, [o.cpu().numpy().astype(np.float64) for o in outs],
+                          [g.cpu().numpy().astype(np.float64) for g in grads])
+    for s in systems:
+        s.close()
+    n_rep, e_rep, g_rep = results["repair"]
+    n_full, e_full, g_full = results["full"]
+    assert n_rep == n_full > results["none"][0]   # "none": refinement-band poses only
+    for a, b in zip(e_rep, e_full):
+        assert (np.abs(a - b) <= 2e-4 + 2.4e-7 * np.abs(b)).all()
+    for a, b in zip(g_rep, g_full):
+        rel = np.linalg.norm(a - b, axis=-1) / np.maximum(np.linalg.norm(b, axis=-1), 1.0)
+        assert rel.max() < 1e-6
