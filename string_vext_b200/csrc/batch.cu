@@ -110,7 +110,7 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
     // symmetric sites (kernels with the per-director border test): q_1 = k0 -
     // m0 t.  All P directors at once with GSUM would spill (slower).
     constexpr bool SYM = BORDER == 2;
-    constexpr int NP = GSUM ? 2 : P;
+    constexpr int NP = GSUM && !SYM ? 2 : P;
     static_assert(P % NP == 0 && (!GSUM || PP <= 2), "director split");
 #pragma unroll 1
     for (int half = 0; half < P / NP; ++half) {
@@ -148,7 +148,7 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
         // acc indices stay compile-time constants (a runtime index would put
         // acc in local memory)
         if constexpr (GSUM) {
-            grad_store<NT>(gsum, a2, NP * half);
+            grad_store<NT, NP, SYM>(gsum, a2, NP * half);
 #pragma unroll
             for (int h = 0; h < P / NP; ++h)
                 if (h == half)
@@ -184,17 +184,17 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
                 const float4 *hb = st.hib + ((seq + c) % kStages) * kCH;
                 constexpr int GNT = GSUM ? NT : 0;
                 if (pass)
-                    far_chunk_adj<P, NEWTON, FLUSH, true, RCP1, UNROLL, GNT, BORDER>(
+                    far_chunk_adj<P, NEWTON, FLUSH, true, RCP1, UNROLL, GNT, BORDER, SYM>(
                         hb, stf, len, g, ux, uy, uz, acc, shift_sum, gsum, border);
                 else
-                    far_chunk_adj<P, NEWTON, FLUSH, false, RCP1, UNROLL, GNT>(
+                    far_chunk_adj<P, NEWTON, FLUSH, false, RCP1, UNROLL, GNT, 0, SYM>(
                         hb, stf, len, g, ux, uy, uz, acc, shift_sum, gsum);
                 stage_next(st, plan, y.hi, y.lo, c, seq);
             }
             seq += plan.n_chunks;
         }
     }
-    if constexpr (GSUM) grad_load<NT>(gsum, acc);
+    if constexpr (GSUM) grad_load<NT, P, SYM>(gsum, acc);
 #pragma unroll
     for (int p = 0; p < P; ++p) {
         const int o = min(obase + G * p, y.O - 1);

@@ -530,7 +530,9 @@ __device__ __forceinline__ void far_chunk_fwd(const float4 *hb, const float4 *st
 //   dE/dc = -6 (sum_s H_s - u sum_s o_s F_s)
 //   dE/du = -6 (sum_s o_s H_s) + (terms along u, removed by the tangent
 //           projection),
-// with H_s = sum_x fp_s d0 and F_s = sum_x fp_s.  AdjAcc holds E, H_s, F_s of
+// with H_s = sum_x fp_s d0 and F_s = sum_x fp_s.  For symmetric sites (o_1 =
+// -o_0) only F_0 - F_1 enters (sum_s o_s F_s = o_0 (F_0 - F_1)): the SYM
+// loops keep it in f[0] and leave f[1] at zero.  AdjAcc holds E, H_s, F_s of
 // one director in FP64.
 struct AdjAcc {
     double e, h[2][3], f[2];
@@ -602,7 +604,8 @@ __device__ __forceinline__ void near_entry_adj(double dx, double dy, double dz, 
             acc[p].h[q][0] = fma(fp, dx, acc[p].h[q][0]);
             acc[p].h[q][1] = fma(fp, dy, acc[p].h[q][1]);
             acc[p].h[q][2] = fma(fp, dz, acc[p].h[q][2]);
-            acc[p].f[q] += fp;
+            if (SYM) acc[p].f[0] += q ? -fp : fp;
+            else acc[p].f[q] += fp;
         }
     }
 }
@@ -649,7 +652,8 @@ __device__ __forceinline__ double &grad_slot(double *gsum, int p, int k) {
 }
 
 // Directors p0 .. p0 + P - 1 of the shared-memory sums from acc.
-template <int NT, int P>
+// (SYM: f[1] stays zero and is neither stored nor loaded.)
+template <int NT, int P, bool SYM = false>
 __device__ __forceinline__ void grad_store(double *gsum, const AdjAcc (&acc)[P], int p0 = 0) {
 #pragma unroll
     for (int p = 0; p < P; ++p)
@@ -658,11 +662,11 @@ __device__ __forceinline__ void grad_store(double *gsum, const AdjAcc (&acc)[P],
 #pragma unroll
             for (int k = 0; k < 3; ++k)
                 grad_slot<NT>(gsum, p0 + p, 3 * q + k) = acc[p].h[q][k];
-            grad_slot<NT>(gsum, p0 + p, 6 + q) = acc[p].f[q];
+            if (!SYM || q == 0) grad_slot<NT>(gsum, p0 + p, 6 + q) = acc[p].f[q];
         }
 }
 
-template <int NT, int P>
+template <int NT, int P, bool SYM = false>
 __device__ __forceinline__ void grad_load(double *gsum, AdjAcc (&acc)[P]) {
 #pragma unroll
     for (int p = 0; p < P; ++p)
@@ -670,7 +674,7 @@ __device__ __forceinline__ void grad_load(double *gsum, AdjAcc (&acc)[P]) {
         for (int q = 0; q < 2; ++q) {
 #pragma unroll
             for (int k = 0; k < 3; ++k) acc[p].h[q][k] = grad_slot<NT>(gsum, p, 3 * q + k);
-            acc[p].f[q] = grad_slot<NT>(gsum, p, 6 + q);
+            if (!SYM || q == 0) acc[p].f[q] = grad_slot<NT>(gsum, p, 6 + q);
         }
 }
 
@@ -695,7 +699,7 @@ __device__ __forceinline__ void grad_load(double *gsum, AdjAcc (&acc)[P]) {
 // Shell entries beyond every site's cutoff are skipped (they add exactly
 // nothing).
 template <int P, bool NEWTON, int FLUSH, bool MASK, bool RCP1 = true, int UNROLL = 1,
-          int GSUM_NT = 0, int BORDER = 0>
+          int GSUM_NT = 0, int BORDER = 0, bool SYM = false>
 __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *stf, int len,
                                               const FarGeom &g, const float2 (&ux)[P / 2],
                                               const float2 (&uy)[P / 2],
@@ -805,7 +809,11 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
                     fh[j][q][0] = __ffma2_rn(fp, dx2, fh[j][q][0]);
                     fh[j][q][1] = __ffma2_rn(fp, dy2, fh[j][q][1]);
                     fh[j][q][2] = __ffma2_rn(fp, dz2, fh[j][q][2]);
-                    ff[j][q] = __fadd2_rn(fp, ff[j][q]);
+                    if (SYM)   // F_0 - F_1 in ff[j][0]
+                        ff[j][0] = q ? __ffma2_rn(fp, make_float2(-1.f, -1.f), ff[j][0])
+                                     : __fadd2_rn(fp, ff[j][0]);
+                    else
+                        ff[j][q] = __fadd2_rn(fp, ff[j][q]);
                 }
             }
         }
@@ -827,8 +835,9 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
                         for (int k = 0; k < 3; ++k)
                             grad_slot<GSUM_NT>(gsum, 2 * j + l, 3 * q + k) +=
                                 (double)(l ? fh[j][q][k].y : fh[j][q][k].x);
-                        grad_slot<GSUM_NT>(gsum, 2 * j + l, 6 + q) +=
-                            (double)(l ? ff[j][q].y : ff[j][q].x);
+                        if (!SYM || q == 0)
+                            grad_slot<GSUM_NT>(gsum, 2 * j + l, 6 + q) +=
+                                (double)(l ? ff[j][q].y : ff[j][q].x);
                     }
         } else {
 #pragma unroll
@@ -836,8 +845,10 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
                 AdjAcc &a0 = acc[2 * j], &a1 = acc[2 * j + 1];
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
-                    a0.f[q] += (double)ff[j][q].x;
-                    a1.f[q] += (double)ff[j][q].y;
+                    if (!SYM || q == 0) {
+                        a0.f[q] += (double)ff[j][q].x;
+                        a1.f[q] += (double)ff[j][q].y;
+                    }
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
                         a0.h[q][k] += (double)fh[j][q][k].x;
