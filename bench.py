@@ -714,12 +714,16 @@ def bench_batch(args, size, axes, device, stream, adjoint=False):
     from string_vext_b200.system import VextBatch, VextSystem
     t0 = time.perf_counter()
     systems = [VextSystem(c) for c in synth.batch_frameworks()]
+    t_sys = time.perf_counter()
     shape = (len(axes), size, size, size)
     outs = [torch.empty(shape, dtype=torch.float32, device=device) for _ in systems]
     grads = ([torch.empty(shape + (6,), dtype=torch.float32, device=device) for _ in systems]
              if adjoint else None)
+    torch.cuda.synchronize()
+    t_out = time.perf_counter()
     batch = VextBatch(systems, size, axes, outs, gradients=grads)
-    setup_s = time.perf_counter() - t0
+    t_batch = time.perf_counter()
+    setup_s = t_batch - t_out   # region lists, work queue, autotuning, graph capture
     info = batch.info()
     t1 = time.perf_counter()
     batch.run(stream)
@@ -740,8 +744,10 @@ def bench_batch(args, size, axes, device, stream, adjoint=False):
     result = {"value": info["poses"] / (ms * 1e-3), "unit": "poses/s", "ms_per_batch": ms,
               "fields": len(systems), "poses": info["poses"], "work_items": info["work_items"],
               "list_gb": info["list_bytes"] / 1e9, "setup_s": setup_s,
-              "cold": {"value": info["poses"] / (setup_s + first_run_s), "unit": "poses/s",
-                       "seconds": setup_s + first_run_s,
+              "setup_parts_s": {"systems": t_sys - t0, "outputs": t_out - t_sys,
+                                "batch": setup_s},
+              "cold": {"value": info["poses"] / (t_batch - t0 + first_run_s), "unit": "poses/s",
+                       "seconds": t_batch - t0 + first_run_s,
                        "path": "systems created, region lists (one set per framework, shared "
                                "by its two guests), autotuning, graph capture and the first "
                                "replay; outputs on the device; host clock"},

@@ -18,7 +18,7 @@
 // or 256 threads x 2, register-resident or shared-memory gradient sums, far
 // entry loop unrolled once or twice) and the number of resident CTAs per SM
 // are chosen by timing each candidate twice on a strided sample of the queue
-// (stride n / (16 x SMs), clamped to 1..64) at creation; the winner is kept
+// (stride n / (16 x SMs), clamped to 1..128) at creation; the winner is kept
 // per (device, kind, size class) so later batches of that class skip the
 // timing, and is captured into the graph.  The batch
 // keeps pointers to its systems' region lists: the systems must outlive it
@@ -785,6 +785,12 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
         VEXT_TRY(get_field_regions(sys, size, cb, b->opt.r_split, &lists[k], sys->stream));
         b->list_bytes += lists[k]->n_entries * 32;
     }
+    {
+        size_t n = 0;
+        for (int k = 0; k < n_systems; ++k)
+            n += (size_t)lists[owner[k]]->n_regions * ((n_axes + kOB - 1) / kOB);
+        items.reserve(n);
+    }
     for (int k = 0; k < n_systems; ++k) {
         System *sys = &systems[k]->sys;
         if (sys->device != dev)
@@ -830,25 +836,30 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
         y.out64 = outputs_f64 ? outputs_f64[k] : nullptr;
         b->max_types = std::max(b->max_types, sys->n_types);
         b->poses += S3 * n_axes;
+        const int n_ob = (n_axes + kOB - 1) / kOB;
         for (int ri = 0; ri < rs->n_regions; ++ri)
-            for (int ob = 0; ob < (n_axes + kOB - 1) / kOB; ++ob)
+            for (int ob = 0; ob < n_ob; ++ob)
                 items.push_back({(long long)rs->h_info[ri].n_total, make_int4(k, ri, ob, 0)});
     }
-    // longest items first
-    std::stable_sort(items.begin(), items.end(),
-                     [](const auto &x, const auto &y) { return x.first > y.first; });
+    // longest items first: a counting sort on the list length (stable, O(n);
+    // the 100-field batches hold 2.7 M items)
+    long long max_len = 0;
+    for (const auto &it : items) max_len = std::max(max_len, it.first);
+    std::vector<int64_t> start((size_t)max_len + 2, 0);
+    for (const auto &it : items) ++start[(size_t)(max_len - it.first) + 1];
+    for (size_t l = 1; l < start.size(); ++l) start[l] += start[l - 1];
     std::vector<int4> hitems(items.size());
-    for (size_t i = 0; i < items.size(); ++i) hitems[i] = items[i].second;
+    for (const auto &it : items) hitems[(size_t)start[(size_t)(max_len - it.first)]++] = it.second;
     b->n_items = (int)hitems.size();
     // the tuning sample: a strided subset of the queue (so it keeps the mix of
-    // long and short items), every 64th item for large queues but at least 16
-    // items per SM, so that the persistent CTAs stay busy while it is timed;
-    // each candidate is timed twice and keeps its better time
+    // long and short items), every 128th item for large queues but at least
+    // 16 items per SM, so that the persistent CTAs stay busy while it is
+    // timed; each candidate is timed twice and keeps its better time
     int sms = 0;
     VEXT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const size_t n_all = hitems.size();
     const size_t stride =
-        std::max<size_t>(1, std::min<size_t>(64, n_all / std::max<size_t>(1, (size_t)sms * 16)));
+        std::max<size_t>(1, std::min<size_t>(128, n_all / std::max<size_t>(1, (size_t)sms * 16)));
     std::vector<int4> sample;
     for (size_t i = 0; i < n_all; i += stride) sample.push_back(hitems[i]);
     b->n_sample = (int)sample.size();
