@@ -13,7 +13,9 @@
 // projected onto the tangent space of the unit quaternion sphere, with
 // u = R(q) e_x = (1 - 2(y^2 + z^2), 2(xy + wz), 2(xz - wy)).
 // Precision follows the field kernel: near chunks FP64, far chunks FP32 with
-// periodic FP64 flushes, FP64 re-evaluation of poses in the refinement band.
+// periodic FP64 flushes, FP64 re-evaluation of poses in the refinement band
+// and of poses with a shell pair within kBorderTol of the cutoff (where the
+// FP32 and FP64 cutoff tests may disagree).
 #include <algorithm>
 #include <cmath>
 
@@ -150,13 +152,13 @@ __global__ void pose_scatter_kernel(PoseArgs a) {
     a.order[a.starts[b] + atomicAdd(&a.cursor[b], 1)] = p;
 }
 
-__device__ __forceinline__ void write_pose(const PoseArgs &a, int p, double e, const double *F0,
-                                           const double *F1) {
+// Outputs of pose p from its energy, dE/dcenter (gc3) and dE/du (gu3, not
+// projected): dE/dq = J(q)^T dE/du, projected on the tangent space of |q| = 1.
+__device__ __forceinline__ void write_pose_sums(const PoseArgs &a, int p, double e,
+                                                const double *gc3, const double *gu) {
     if (a.energy) a.energy[p] = e;
     if (a.gc)
-        for (int k = 0; k < 3; ++k) a.gc[3 * p + k] = F0[k] + F1[k];
-    double gu[3];
-    for (int k = 0; k < 3; ++k) gu[k] = a.off0 * F0[k] + a.off1 * F1[k];
+        for (int k = 0; k < 3; ++k) a.gc[3 * p + k] = gc3[k];
     if (a.gu)
         for (int k = 0; k < 3; ++k) a.gu[3 * p + k] = gu[k];
     if (a.gq) {
@@ -176,6 +178,18 @@ __device__ __forceinline__ void write_pose(const PoseArgs &a, int p, double e, c
     }
 }
 
+// The same from the two site forces F0, F1 (dE/dcenter = F0 + F1, dE/du =
+// o0 F0 + o1 F1).
+__device__ __forceinline__ void write_pose(const PoseArgs &a, int p, double e, const double *F0,
+                                           const double *F1) {
+    double gc[3], gu[3];
+    for (int k = 0; k < 3; ++k) {
+        gc[k] = F0[k] + F1[k];
+        gu[k] = a.off0 * F0[k] + a.off1 * F1[k];
+    }
+    write_pose_sums(a, p, e, gc, gu);
+}
+
 // Far entries [e_begin, e_end) of one staged chunk for one pose: the packed
 // FP32x2 loop of the field kernels with the lanes holding the pose's two
 // sites.  Per lane d = x - r_s, n1 = hardware reciprocal of d2, n3 = n1^3,
@@ -185,12 +199,14 @@ __device__ __forceinline__ void write_pose(const PoseArgs &a, int p, double e, c
 // MASK = false for inner entries (inside the cutoff of every such site): no
 // cutoff mask, and the shift is summed once per entry into shift_sum (added
 // to both sites).  Energy partials are flushed into FP64 every 16 entries,
-// the gradient partials once per call.
+// the gradient partials once per call.  MASK: bmin (per site) receives the
+// smallest |d2 - rc^2| met, for the FP64 re-evaluation of poses with a pair
+// too close to the cutoff for the FP32 test (kBorderTol).
 template <bool MASK>
 __device__ __forceinline__ void pose_far(const float4 *hb, const float4 *stf, int e_begin,
                                          int e_end, float2 nsx, float2 nsy, float2 nsz,
                                          float rc2f, double (&E)[2], double (&F)[2][3],
-                                         double &shift_sum) {
+                                         double &shift_sum, float2 &bmin) {
     float2 gx = make_float2(0.f, 0.f), gy = gx, gz = gx;
 #pragma unroll 1
     for (int e0 = e_begin; e0 < e_end; e0 += 16) {
@@ -223,6 +239,9 @@ __device__ __forceinline__ void pose_far(const float4 *hb, const float4 *stf, in
                 const float2 m = make_float2(set_lt(d2.x, rc2f), set_lt(d2.y, rc2f));
                 n3 = __fmul2_rn(n3, m);
                 fe = __ffma2_rn(m, sh, fe);
+                const float2 x = __fadd2_rn(d2, make_float2(-rc2f, -rc2f));
+                bmin.x = fminf(bmin.x, fabsf(x.x));
+                bmin.y = fminf(bmin.y, fabsf(x.y));
             }
             fe = __ffma2_rn(n3, __ffma2_rn(c12, n3, mc6), fe);
             const float2 fp = __fmul2_rn(__fmul2_rn(n1, n3), __ffma2_rn(m2c12, n3, c6));
@@ -288,6 +307,7 @@ __global__ void __launch_bounds__(NT) pose_kernel(PoseArgs a) {
     const double ux = a.u[3 * p], uy = a.u[3 * p + 1], uz = a.u[3 * p + 2];
     double sd[2][3];
     double E[2] = {0, 0}, F[2][3] = {{0, 0, 0}, {0, 0, 0}}, shift_sum = 0.0;
+    float2 bmin = make_float2(__int_as_float(0x7f800000), __int_as_float(0x7f800000));
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
         const double off = s ? a.off1 : a.off0;
@@ -375,8 +395,8 @@ __global__ void __launch_bounds__(NT) pose_kernel(PoseArgs a) {
             const float4 *hb = st.hib + s * kCH;
             const int split = min(max(r.n_near + r.n_inner - start, 0), len);
             if (warp_on) {
-                pose_far<false>(hb, stf, 0, split, nsx, nsy, nsz, a.rc2f, E, F, shift_sum);
-                pose_far<true>(hb, stf, split, len, nsx, nsy, nsz, a.rc2f, E, F, shift_sum);
+                pose_far<false>(hb, stf, 0, split, nsx, nsy, nsz, a.rc2f, E, F, shift_sum, bmin);
+                pose_far<true>(hb, stf, split, len, nsx, nsy, nsz, a.rc2f, E, F, shift_sum, bmin);
             }
         }
         __syncthreads();
@@ -386,14 +406,18 @@ __global__ void __launch_bounds__(NT) pose_kernel(PoseArgs a) {
     if (valid) {
         const double e = E[0] + E[1] + 2.0 * shift_sum;
         write_pose(a, p, e, F[0], F[1]);
-        if (a.refine && e > a.band_lo && e < a.band_hi) {
+        // the refinement band, or a shell pair within kBorderTol of the cutoff
+        if (a.refine && ((e > a.band_lo && e < a.band_hi) || fminf(bmin.x, bmin.y) < kBorderTol)) {
             const int k = atomicAdd(&a.refine[0], 1);
             a.refine[1 + k] = p;
         }
     }
 }
 
-// FP64 re-evaluation of flagged poses, one warp per pose.
+// FP64 re-evaluation of flagged poses, one warp per pose: the pair test and
+// terms of the FP64 pose sums (fp64_pose_pairs_both: both sites per entry,
+// the reciprocal from the hardware seed and two Newton steps), the lanes
+// striding over the bin's list.
 __global__ void pose_refine_kernel(PoseArgs a) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -405,38 +429,17 @@ __global__ void pose_refine_kernel(PoseArgs a) {
         double cx, cy, cz;
         frac_to_cart(a.H, a.wf[3 * p] - r.of[0], a.wf[3 * p + 1] - r.of[1],
                      a.wf[3 * p + 2] - r.of[2], cx, cy, cz);
-        const double ux = a.u[3 * p], uy = a.u[3 * p + 1], uz = a.u[3 * p + 2];
-        double v[7] = {0, 0, 0, 0, 0, 0, 0};   // E, F0 (3), F1 (3)
-        for (int s = 0; s < 2; ++s) {
-            const double off = s ? a.off1 : a.off0;
-            const double px = cx + off * ux, py = cy + off * uy, pz = cz + off * uz;
-            for (int e = lane; e < r.n_total; e += 32) {
-                const float4 h = a.hi[r.off + e], l = a.lo[r.off + e];
-                const double dx = px - ((double)h.x + (double)l.x);
-                const double dy = py - ((double)h.y + (double)l.y);
-                const double dz = pz - ((double)h.z + (double)l.z);
-                const double d2 = dx * dx + dy * dy + dz * dz;
-                if (d2 >= a.rc2) continue;
-                const int t = __float_as_int(h.w);
-                const double c12 = a.td[4 * t], c6 = a.td[4 * t + 1], shift = a.td[4 * t + 2],
-                             fl = a.td[4 * t + 3];
-                const double s2 = d2 < fl ? fl : d2;
-                const double i2 = 1.0 / s2;
-                const double i6 = i2 * i2 * i2;
-                v[0] += c12 * i6 * i6 - c6 * i6 + shift;
-                if (d2 > fl) {
-                    const double w = i2 * i6 * (6.0 * c6 - 12.0 * c12 * i6);
-                    v[1 + 3 * s] += w * dx;
-                    v[2 + 3 * s] += w * dy;
-                    v[3 + 3 * s] += w * dz;
-                }
-            }
+        const double u[3] = {a.u[3 * p], a.u[3 * p + 1], a.u[3 * p + 2]};
+        double e = 0.0, g[6];
+        fp64_pose_pairs_both(a.hi, a.lo, a.td, r.off, r.n_total, lane, 32, a.rc2, a.off0, a.off1,
+                             cx, cy, cz, u, e, g);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            e += __shfl_xor_sync(0xffffffffu, e, o);
+#pragma unroll
+            for (int k = 0; k < 6; ++k) g[k] += __shfl_xor_sync(0xffffffffu, g[k], o);
         }
-#pragma unroll
-        for (int k = 0; k < 7; ++k)
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
-        if (lane == 0) write_pose(a, p, v[0], v + 1, v + 4);
+        if (lane == 0) write_pose_sums(a, p, e, g, g + 3);
     }
 }
 
@@ -541,7 +544,7 @@ int pose_enqueue(System *sys, int n, const double *centers, const double *quats,
     a.tf = sys->d_tf;
     a.td = sys->d_td;
     a.n_types = sys->n_types;
-    const bool refine = o.mode == VEXT_MODE_MIXED && o.band_hi > o.band_lo;
+    const bool refine = o.mode == VEXT_MODE_MIXED;   // band and border poses
     int *d_refine = bump.take<int>((size_t)n + 1);
     a.refine = refine ? d_refine : nullptr;
     a.band_lo = o.band_lo;

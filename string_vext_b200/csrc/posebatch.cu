@@ -9,8 +9,10 @@
 // sites in the two lanes; reciprocal of d^2 per pair, cubed) with per-lane
 // FP32 partials flushed into FP64 every 16 entries.  The seven sums (E,
 // dE/dsite for both sites) are reduced over the warp, then over the pose's
-// warps in shared memory; a pose whose energy falls in the refinement band is
-// recomputed entirely in FP64 by its first warp.  Outputs as
+// warps in shared memory; a pose whose energy falls in the refinement band, or
+// with a shell pair within kBorderTol of the cutoff (where the FP32 and FP64
+// cutoff tests may disagree), is recomputed entirely in FP64 by its first
+// warp.  Outputs as
 // vext_pose_energy_grad: E, dE/dcenter, tangent dE/dq, dE/du.  Pair term and
 // forces as in pose.cu.
 #include <algorithm>
@@ -41,12 +43,12 @@ struct PoseBatchArgs {
 // fp = (n1 n3)(c6 - 2 c12 n3), dE/dsite += -6 fp d.  MASK = false for inner
 // entries (within the cutoff of every pose of the bin: no mask, the shift
 // summed once per entry into shift_sum).  FP32 partials are flushed into the
-// FP64 sums every 16 entries.
+// FP64 sums every 16 entries.  MASK: bmin receives the smallest |d2 - rc^2|.
 template <bool MASK>
 __device__ __forceinline__ void far_lane_sums(const PoseBatchSys &y, long long base, int begin,
                                               int end, int lane, int stride, float2 nsx,
                                               float2 nsy, float2 nsz, double (&v)[7],
-                                              double &shift_sum) {
+                                              double &shift_sum, float &bmin) {
     const int mine = end - begin > lane ? (end - begin - lane + stride - 1) / stride : 0;
 #pragma unroll 1
     for (int i0 = 0; i0 < mine; i0 += 16) {
@@ -69,6 +71,7 @@ __device__ __forceinline__ void far_lane_sums(const PoseBatchSys &y, long long b
                 const float2 m = make_float2(set_lt(d2.x, y.rc2f), set_lt(d2.y, y.rc2f));
                 n3 = __fmul2_rn(n3, m);
                 fe = __ffma2_rn(m, make_float2(tp.z, tp.z), fe);
+                bmin = fminf(bmin, fminf(fabsf(d2.x - y.rc2f), fabsf(d2.y - y.rc2f)));
             } else {
                 fs += tp.z;
             }
@@ -102,7 +105,7 @@ __device__ __forceinline__ void far_lane_sums(const PoseBatchSys &y, long long b
 template <bool FAR64>
 __device__ __forceinline__ void pose_sums(const PoseBatchSys &y, const RegionInfo &r,
                                           const double (&sd)[2][3], int lane, int stride,
-                                          double (&v)[7]) {
+                                          double (&v)[7], float &bmin) {
     for (int e = lane; e < (FAR64 ? r.n_total : r.n_near); e += stride) {
         const float4 h = y.hi[r.off + e], l = y.lo[r.off + e];
         const double x = (double)h.x + (double)l.x, yy = (double)h.y + (double)l.y,
@@ -135,9 +138,9 @@ __device__ __forceinline__ void pose_sums(const PoseBatchSys &y, const RegionInf
                  nsz = make_float2(-(float)sd[0][2], -(float)sd[1][2]);
     double shift_sum = 0.0;
     far_lane_sums<false>(y, r.off, r.n_near, r.n_near + r.n_inner, lane, stride, nsx, nsy, nsz,
-                         v, shift_sum);
+                         v, shift_sum, bmin);
     far_lane_sums<true>(y, r.off, r.n_near + r.n_inner, r.n_total, lane, stride, nsx, nsy, nsz,
-                        v, shift_sum);
+                        v, shift_sum, bmin);
     v[0] += 2.0 * shift_sum;
 }
 
@@ -154,7 +157,7 @@ __device__ __forceinline__ void warp_reduce7(double (&v)[7]) {
 // the FP64 mode (every entry near, evaluated as in refinement).
 template <bool MIXED>
 __global__ void __launch_bounds__(256) pose_batch_kernel(PoseBatchArgs a) {
-    __shared__ double part[8][7];
+    __shared__ double part[8][8];   // 7 sums and the border distance per warp
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int W = a.wpp, per_cta = 8 / W, sub = warp % W;
     const long long groups = (a.n + per_cta - 1) / per_cta;
@@ -203,12 +206,17 @@ __global__ void __launch_bounds__(256) pose_batch_kernel(PoseBatchArgs a) {
             sd[s][2] = cz + off * u[2];
         }
         double v[7] = {0, 0, 0, 0, 0, 0, 0};
-        pose_sums<!MIXED>(y, r, sd, lane + 32 * sub, 32 * W, v);
+        float bmin = __int_as_float(0x7f800000);
+        pose_sums<!MIXED>(y, r, sd, lane + 32 * sub, 32 * W, v, bmin);
         warp_reduce7(v);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) bmin = fminf(bmin, __shfl_xor_sync(0xffffffffu, bmin, o));
         if (W > 1) {   // (W is a launch argument: uniform over the CTA)
-            if (lane == 0)
+            if (lane == 0) {
 #pragma unroll
                 for (int k = 0; k < 7; ++k) part[warp][k] = v[k];
+                part[warp][7] = (double)bmin;
+            }
             __syncthreads();
             const int w0 = warp - sub;
 #pragma unroll
@@ -217,13 +225,16 @@ __global__ void __launch_bounds__(256) pose_batch_kernel(PoseBatchArgs a) {
                 for (int j = 1; j < W; ++j) t += part[w0 + j][k];
                 v[k] = t;
             }
+            for (int j = 0; j < W; ++j) bmin = fminf(bmin, (float)part[w0 + j][7]);
             __syncthreads();
         }
         if (sub != 0) continue;
-        if (MIXED && v[0] > a.band_lo && v[0] < a.band_hi) {   // warp-uniform: all lanes hold it
+        // warp-uniform: all lanes hold v[0] and bmin
+        if (MIXED && ((v[0] > a.band_lo && v[0] < a.band_hi) || bmin < kBorderTol)) {
 #pragma unroll
             for (int k = 0; k < 7; ++k) v[k] = 0.0;
-            pose_sums<true>(y, r, sd, lane, 32, v);
+            float unused = 0.f;
+            pose_sums<true>(y, r, sd, lane, 32, v, unused);
             warp_reduce7(v);
         }
         if (live && lane == 0) {
