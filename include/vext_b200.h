@@ -73,8 +73,10 @@ VEXT_API int evaluate_reused_neighbors(int n_centers, int n_axes, int n_images, 
  * pose) return VEXT_ERR_CAPACITY before anything is copied to the device.
  * The first call on each device loads the library's module there; every
  * call looks the array's device address up with cudaGetSymbolAddress.  Work
- * runs on the calling thread's per-thread default stream and is finished
- * when the call returns; calls are serialised inside the process.  The array
+ * runs eagerly on the calling thread's per-thread default stream and is
+ * finished when the call returns (it synchronises that stream, so it is not
+ * to be called while that stream is being captured); calls are serialised
+ * inside the process.  The array
  * keeps the last call's contents, and calls that overlapped on the GPU would
  * race on it. */
 VEXT_API int evaluate_reused_neighbors_noalloc(int n_centers, int n_axes, int n_images,
