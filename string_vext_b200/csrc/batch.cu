@@ -871,12 +871,13 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
     const int size_class =
         (int)std::lround(std::log2(std::max(mean_len, 1.0))) * 64 +
         (int)std::lround(std::log2((double)std::max<size_t>(items.size(), 1)));
-    // the per-director border test of kind 6 assumes symmetric sites (o_1 =
-    // -o_0 != 0); other guests take the same shapes with the per-site test
+    // kind 6 (the per-director border test, q_1 from the site-0 terms)
+    // assumes exactly symmetric sites, o_1 = -o_0 != 0 (two identical sites
+    // about their center of mass); other guests take the same shapes with the
+    // per-site test and both sites' terms
     if (b->kind == 6)
         for (const BatchSys &y : hs)
-            if (y.off0 == 0.0 || std::fabs(y.off0 + y.off1) > 1e-9 * std::fabs(y.off0 - y.off1))
-                b->kind = 9;
+            if (y.off0 == 0.0 || y.off1 != -y.off0) b->kind = 9;
     for (const BatchSys &y : hs) b->targets.push_back({y.out, y.grad});
     VEXT_CUDA(cudaMalloc(&b->d_sys, sizeof(BatchSys) * n_systems));
     VEXT_CUDA(cudaMemcpy(b->d_sys, hs.data(), sizeof(BatchSys) * n_systems, cudaMemcpyHostToDevice));

@@ -740,7 +740,7 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
                 const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                 if (MASK && dd > g.out2) continue;
                 k0 = make_float2(dd + g.oo0, dd + g.oo0);
-                k1 = make_float2(dd + g.oo1, dd + g.oo1);
+                if (!SYM) k1 = make_float2(dd + g.oo1, dd + g.oo1);   // SYM: o_1^2 = o_0^2
                 dx2 = make_float2(dx, dx);
                 dy2 = make_float2(dy, dy);
                 dz2 = make_float2(dz, dz);
@@ -762,7 +762,7 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
                 }
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
-                    const float2 d2 = __ffma2_rn(q ? g.m1 : g.m0, t, q ? k1 : k0);
+                    const float2 d2 = __ffma2_rn(q ? g.m1 : g.m0, t, q && !SYM ? k1 : k0);
                     float2 fp;
                     if (RCP1) {
                         float r0, r1;
