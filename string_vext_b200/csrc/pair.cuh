@@ -331,6 +331,26 @@ constexpr float kBorderTol = 1.25e-4f;
 // q's own distance, so the director test flags below kBorderTol + 4e-5.
 constexpr float kBorderTolDir = kBorderTol + 4e-5f;
 
+// One far (site, atom) pair in FP64 for a site whose FP32 d2 lies within
+// kBorderTol of rc^2: the oracle's test (d2 >= rc^2 out) decides it; inside,
+// its energy (with the shift) is added to e and its site force dE/dsite =
+// 2 (dE/dd2) (site - x) to f.  Far pairs lie beyond every contact floor.
+__device__ __forceinline__ void fp64_border_pair(double sx, double sy, double sz, double ax,
+                                                 double ay, double az, const double *td, int ty,
+                                                 double rc2, double &e, double *f) {
+    const double dx = sx - ax, dy = sy - ay, dz = sz - az;
+    const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
+    if (d2 >= rc2) return;
+    const double c12 = td[4 * ty], c6 = td[4 * ty + 1];
+    const double i2 = rcp64_nr<2>(d2);
+    const double i6 = i2 * i2 * i2;
+    e += fma(i6, fma(c12, i6, -c6), td[4 * ty + 2]);
+    const double w = i2 * i6 * fma(-12.0 * c12, i6, 6.0 * c6);
+    f[0] = fma(w, dx, f[0]);
+    f[1] = fma(w, dy, f[1]);
+    f[2] = fma(w, dz, f[2]);
+}
+
 // Border repair of one pose (entries k = first, first + step, ... of the
 // shell range [off, off + n) of its region list): for each site, the far
 // kernel's FP32 inside/outside decision -- recomputed with exactly its

@@ -9,10 +9,10 @@
 // sites in the two lanes; reciprocal of d^2 per pair, cubed) with per-lane
 // FP32 partials flushed into FP64 every 16 entries.  The seven sums (E,
 // dE/dsite for both sites) are reduced over the warp, then over the pose's
-// warps in shared memory; a pose whose energy falls in the refinement band, or
-// with a shell pair within kBorderTol of the cutoff (where the FP32 and FP64
-// cutoff tests may disagree), is recomputed entirely in FP64 by its first
-// warp.  Outputs as
+// warps in shared memory; a pose whose energy falls in the refinement band is
+// recomputed entirely in FP64 by its warps.  Shell pairs whose FP32 d2 lies
+// within kBorderTol of the cutoff (where the FP32 and FP64 cutoff tests may
+// disagree) are taken in FP64 on the spot.  Outputs as
 // vext_pose_energy_grad: E, dE/dcenter, tangent dE/dq, dE/du.  Pair term and
 // forces as in pose.cu.
 #include <algorithm>
@@ -43,12 +43,15 @@ struct PoseBatchArgs {
 // fp = (n1 n3)(c6 - 2 c12 n3), dE/dsite += -6 fp d.  MASK = false for inner
 // entries (within the cutoff of every pose of the bin: no mask, the shift
 // summed once per entry into shift_sum).  FP32 partials are flushed into the
-// FP64 sums every 16 entries.  MASK: bmin receives the smallest |d2 - rc^2|.
+// FP64 sums every 16 entries.  MASK: a site whose FP32 d2 lies within
+// kBorderTol of rc^2 -- where the FP32 test might decide the pair unlike the
+// FP64 one -- leaves the FP32 sums and takes the pair in FP64
+// (fp64_border_pair, from the hi + lo position and the FP64 site sd).
 template <bool MASK>
 __device__ __forceinline__ void far_lane_sums(const PoseBatchSys &y, long long base, int begin,
                                               int end, int lane, int stride, float2 nsx,
-                                              float2 nsy, float2 nsz, double (&v)[7],
-                                              double &shift_sum, float &bmin) {
+                                              float2 nsy, float2 nsz, const double (&sd)[2][3],
+                                              double (&v)[7], double &shift_sum) {
     const int mine = end - begin > lane ? (end - begin - lane + stride - 1) / stride : 0;
 #pragma unroll 1
     for (int i0 = 0; i0 < mine; i0 += 16) {
@@ -56,7 +59,8 @@ __device__ __forceinline__ void far_lane_sums(const PoseBatchSys &y, long long b
         float fs = 0.f;
         const int i1 = min(i0 + 16, mine);
         for (int i = i0; i < i1; ++i) {
-            const float4 h = y.hi[base + begin + lane + (long long)stride * i];
+            const long long k = base + begin + lane + (long long)stride * i;
+            const float4 h = y.hi[k];
             const float4 tp = y.tf[__float_as_int(h.w)];   // (c12, c6, shift, floor2)
             const float2 dx = __fadd2_rn(make_float2(h.x, h.x), nsx),
                          dy = __fadd2_rn(make_float2(h.y, h.y), nsy),
@@ -68,10 +72,27 @@ __device__ __forceinline__ void far_lane_sums(const PoseBatchSys &y, long long b
             const float2 n1 = make_float2(r0, r1);
             float2 n3 = __fmul2_rn(__fmul2_rn(n1, n1), n1);
             if (MASK) {
-                const float2 m = make_float2(set_lt(d2.x, y.rc2f), set_lt(d2.y, y.rc2f));
+                float2 m = make_float2(set_lt(d2.x, y.rc2f), set_lt(d2.y, y.rc2f));
+                const float2 x = __fadd2_rn(d2, make_float2(-y.rc2f, -y.rc2f));
+                const bool b0 = fabsf(x.x) < kBorderTol, b1 = fabsf(x.y) < kBorderTol;
+                if (b0 || b1) {   // rare
+                    const float4 l = y.lo[k];
+                    const double ax = (double)h.x + (double)l.x, ay = (double)h.y + (double)l.y,
+                                 az = (double)h.z + (double)l.z;
+                    const int ty = __float_as_int(h.w);
+                    if (b0) {
+                        m.x = 0.f;
+                        fp64_border_pair(sd[0][0], sd[0][1], sd[0][2], ax, ay, az, y.td, ty, y.rc2,
+                                         v[0], v + 1);
+                    }
+                    if (b1) {
+                        m.y = 0.f;
+                        fp64_border_pair(sd[1][0], sd[1][1], sd[1][2], ax, ay, az, y.td, ty, y.rc2,
+                                         v[0], v + 4);
+                    }
+                }
                 n3 = __fmul2_rn(n3, m);
                 fe = __ffma2_rn(m, make_float2(tp.z, tp.z), fe);
-                bmin = fminf(bmin, fminf(fabsf(d2.x - y.rc2f), fabsf(d2.y - y.rc2f)));
             } else {
                 fs += tp.z;
             }
@@ -98,14 +119,15 @@ __device__ __forceinline__ void far_lane_sums(const PoseBatchSys &y, long long b
 
 // Sums of one pose over its bin list: v = (E, dE/dsite0 [3], dE/dsite1 [3]),
 // partial over the entries lane, lane + stride, ... (reduced by the caller).  FAR64 evaluates every entry in FP64
-// with the correctly rounded reciprocal (refinement, and the FP64 mode whose
-// entries are all near); otherwise near entries in FP64 with the hardware
-// reciprocal seed + one Newton step (relative error <= 2^-46) and far entries
-// in packed FP32.
-template <bool FAR64>
+// (the FP64 mode, whose entries are all near, with the correctly rounded
+// reciprocal; the re-evaluation of flagged poses, IEEE = false, with the
+// hardware seed + two Newton steps, within an ulp or two of it); otherwise
+// near entries in FP64 with the hardware reciprocal seed + one Newton step
+// (relative error <= 2^-46) and far entries in packed FP32.
+template <bool FAR64, bool IEEE = FAR64>
 __device__ __forceinline__ void pose_sums(const PoseBatchSys &y, const RegionInfo &r,
                                           const double (&sd)[2][3], int lane, int stride,
-                                          double (&v)[7], float &bmin) {
+                                          double (&v)[7]) {
     for (int e = lane; e < (FAR64 ? r.n_total : r.n_near); e += stride) {
         const float4 h = y.hi[r.off + e], l = y.lo[r.off + e];
         const double x = (double)h.x + (double)l.x, yy = (double)h.y + (double)l.y,
@@ -119,7 +141,7 @@ __device__ __forceinline__ void pose_sums(const PoseBatchSys &y, const RegionInf
             const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
             if (d2 >= y.rc2) continue;
             const double s2 = d2 < fl ? fl : d2;
-            const double i2 = FAR64 ? 1.0 / s2 : rcp64_nr<1>(s2);
+            const double i2 = IEEE ? 1.0 / s2 : FAR64 ? rcp64_nr<2>(s2) : rcp64_nr<1>(s2);
             const double i6 = i2 * i2 * i2;
             v[0] += fma(i6, fma(c12, i6, -c6), shift);
             if (d2 > fl) {
@@ -138,9 +160,9 @@ __device__ __forceinline__ void pose_sums(const PoseBatchSys &y, const RegionInf
                  nsz = make_float2(-(float)sd[0][2], -(float)sd[1][2]);
     double shift_sum = 0.0;
     far_lane_sums<false>(y, r.off, r.n_near, r.n_near + r.n_inner, lane, stride, nsx, nsy, nsz,
-                         v, shift_sum, bmin);
+                         sd, v, shift_sum);
     far_lane_sums<true>(y, r.off, r.n_near + r.n_inner, r.n_total, lane, stride, nsx, nsy, nsz,
-                        v, shift_sum, bmin);
+                        sd, v, shift_sum);
     v[0] += 2.0 * shift_sum;
 }
 
@@ -157,7 +179,7 @@ __device__ __forceinline__ void warp_reduce7(double (&v)[7]) {
 // the FP64 mode (every entry near, evaluated as in refinement).
 template <bool MIXED>
 __global__ void __launch_bounds__(256) pose_batch_kernel(PoseBatchArgs a) {
-    __shared__ double part[8][8];   // 7 sums and the border distance per warp
+    __shared__ double part[8][7];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int W = a.wpp, per_cta = 8 / W, sub = warp % W;
     const long long groups = (a.n + per_cta - 1) / per_cta;
@@ -206,17 +228,12 @@ __global__ void __launch_bounds__(256) pose_batch_kernel(PoseBatchArgs a) {
             sd[s][2] = cz + off * u[2];
         }
         double v[7] = {0, 0, 0, 0, 0, 0, 0};
-        float bmin = __int_as_float(0x7f800000);
-        pose_sums<!MIXED>(y, r, sd, lane + 32 * sub, 32 * W, v, bmin);
+        pose_sums<!MIXED>(y, r, sd, lane + 32 * sub, 32 * W, v);
         warp_reduce7(v);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) bmin = fminf(bmin, __shfl_xor_sync(0xffffffffu, bmin, o));
         if (W > 1) {   // (W is a launch argument: uniform over the CTA)
-            if (lane == 0) {
+            if (lane == 0)
 #pragma unroll
                 for (int k = 0; k < 7; ++k) part[warp][k] = v[k];
-                part[warp][7] = (double)bmin;
-            }
             __syncthreads();
             const int w0 = warp - sub;
 #pragma unroll
@@ -225,18 +242,36 @@ __global__ void __launch_bounds__(256) pose_batch_kernel(PoseBatchArgs a) {
                 for (int j = 1; j < W; ++j) t += part[w0 + j][k];
                 v[k] = t;
             }
-            for (int j = 0; j < W; ++j) bmin = fminf(bmin, (float)part[w0 + j][7]);
             __syncthreads();
         }
-        if (sub != 0) continue;
-        // warp-uniform: all lanes hold v[0] and bmin
-        if (MIXED && ((v[0] > a.band_lo && v[0] < a.band_hi) || bmin < kBorderTol)) {
+        // the refinement band: the pose again in FP64, by all of its warps
+        // (uniform over them: each holds the pose's v[0])
+        if (MIXED) {
+            const bool again = v[0] > a.band_lo && v[0] < a.band_hi;
+            if (again) {
 #pragma unroll
-            for (int k = 0; k < 7; ++k) v[k] = 0.0;
-            float unused = 0.f;
-            pose_sums<true>(y, r, sd, lane, 32, v, unused);
-            warp_reduce7(v);
+                for (int k = 0; k < 7; ++k) v[k] = 0.0;
+                pose_sums<true, false>(y, r, sd, lane + 32 * sub, 32 * W, v);
+                warp_reduce7(v);
+            }
+            if (W > 1) {   // every warp of the CTA passes both barriers
+                if (again && lane == 0)
+#pragma unroll
+                    for (int k = 0; k < 7; ++k) part[warp][k] = v[k];
+                __syncthreads();
+                if (again) {
+                    const int w0 = warp - sub;
+#pragma unroll
+                    for (int k = 0; k < 7; ++k) {
+                        double t = part[w0][k];
+                        for (int j = 1; j < W; ++j) t += part[w0 + j][k];
+                        v[k] = t;
+                    }
+                }
+                __syncthreads();
+            }
         }
+        if (sub != 0) continue;
         if (live && lane == 0) {
             if (a.energy) a.energy[p] = v[0];
             double gu[3];
