@@ -425,3 +425,40 @@ def test_border_repair_matches_full_fp64_refinement():
     for a, b in zip(g_rep, g_full):
         rel = np.linalg.norm(a - b, axis=-1) / np.maximum(np.linalg.norm(b, axis=-1), 1.0)
         assert rel.max() < 1e-6
+
+
+def test_asymmetric_guest_takes_the_per_site_kernels():
+    """Two identical sites of unequal mass sit off-center (o_1 != -o_0): the
+    batch then runs the kernels that test the cutoff border per site and keep
+    both sites' terms (the symmetric shortcuts do not apply).  Energies and
+    gradients of every pose (small_field and a batch framework, 12^3 x 64)
+    within the bar of the plain FP64 adjoint."""
+    for case in (synth.small_field(), synth.batch_frameworks(1)[0]):
+        case = dict(case)
+        case["guest_mass"] = np.array([15.0, 25.0])
+        case["total_mass"] = 40.0
+        size = 12
+        _, axes = regular_pose_grid(size, 64)
+        axes = normalized_directors(axes)
+        shape = (64, size, size, size)
+        with VextSystem(case) as system:
+            off = system.offsets
+            assert off[0] != -off[1]
+            out = torch.empty(shape, dtype=torch.float32, device="cuda")
+            grad = torch.empty(shape + (6,), dtype=torch.float32, device="cuda")
+            batch = VextBatch([system], size, axes, [out], gradients=[grad])
+            assert "border/site" in batch.info()["cta_shape"]
+            batch.run()
+            batch.check()
+            batch.close()
+            e64 = torch.empty(shape, dtype=torch.float64, device="cuda")
+            g64 = torch.empty(shape + (6,), dtype=torch.float64, device="cuda")
+            system.field_adjoint_device(size, axes, None, None, e64, g64,
+                                        mode=_lib.VEXT_MODE_FP64_PLAIN)
+            torch.cuda.synchronize()
+        ex, gx = e64.cpu().numpy(), g64.cpu().numpy()
+        got = out.cpu().numpy().astype(np.float64)
+        assert (np.abs(got - ex) <= 1e-4 + 1.2e-7 * np.abs(ex)).all()
+        gm = grad.cpu().numpy().astype(np.float64)
+        grel = np.linalg.norm(gm - gx, axis=-1) / np.maximum(np.linalg.norm(gx, axis=-1), 1.0)
+        assert grel.max() < 1e-5

@@ -225,3 +225,24 @@ def test_pairs_at_the_cutoff_are_decided_in_fp64(length, n_random):
     assert np.abs(e[:64] - e64).max() < 1e-6
     assert np.abs(gc[:64] - gc64).max() < 1e-6
     assert np.abs(gq[:64] - gq64).max() < 1e-6
+
+
+def test_asymmetric_guest_pose_path():
+    """Unequal site masses put the sites off-center (o_1 != -o_0); the pose
+    kernels carry each site's offset: FP64 mode against the oracle, mixed
+    against FP64 mode within the bar, on random poses (warp-per-pose path)."""
+    case = dict(synth.small_field())
+    case["guest_mass"] = np.array([15.0, 25.0])
+    case["total_mass"] = 40.0
+    cart, q = random_poses(case, 512, 23)
+    with VextSystem(case) as system:
+        e, gc, gq, _ = system.pose_energy_grad(cart, q, mode=MIXED)
+        e64, gc64, gq64, gu64 = system.pose_energy_grad(cart, q, mode=FP64)
+    re, rgc, rgu = oracle.pose_energy_grad(case, cart, director(q))
+    np.testing.assert_allclose(e64, re, rtol=1e-10, atol=1e-8)
+    assert (np.abs(gc64 - rgc) / np.maximum(np.abs(rgc).max(axis=1, keepdims=True), 1.0)).max() < 1e-9
+    neg = e64 <= 0
+    assert np.abs(e - e64)[neg].max(initial=0) < 1e-4
+    assert (np.abs(e - e64) / np.maximum(np.abs(e64), 1))[~neg].max() < 1e-6
+    scale = np.maximum(np.linalg.norm(gc64, axis=1), 1.0)
+    assert (np.linalg.norm(gc - gc64, axis=1) / scale).max() < 1e-5
