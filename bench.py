@@ -350,7 +350,7 @@ def run_ours(args, rank, world, local_rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32x2+f64 (pairs < 5 A in FP64, beyond in packed FP32 with FP64-flushed "
                      "partial sums; FP64 energy refinement band; FP64 re-evaluation of poses "
-                     "with a shell pair within 1e-4 A^2 of the cutoff)",
+                     "with a shell pair within the FP32 error of the cutoff)",
             "data": "synthetic", "config": config_of(args.workload, size),
             "step": "forward + adjoint of every pose: energy, dE/d(center), tangent dE/du; "
                     "region lists resident (built once per framework, reported as setup)",

@@ -185,9 +185,9 @@ __device__ __forceinline__ void near_chunk(const double *ed, const double *std4,
 //   e += sum over sites and in-cutoff pairs of c12 i6^2 - c6 i6 + shift,
 //   g[0..2] += dE/dc, g[3..5] += dE/du (not yet projected),
 // with d2 >= rc^2 out (the reference's test, kernel.cpp:29-30), the contact
-// floor on d2 and no force below it.  The same code serves the plain FP64
-// kernels (one thread per pose) and the FP64 re-evaluation of flagged poses
-// (a warp per pose), so both classify every pair identically.
+// floor on d2 and no force below it.  It serves the plain FP64 kernels (one
+// thread per pose); the FP64 re-evaluation of flagged poses (a warp per pose)
+// uses fp64_pose_pairs_both, the same pair test and terms.
 __device__ __forceinline__ void fp64_pose_pairs(const float4 *hi, const float4 *lo,
                                                 const double *td, long long off, int n,
                                                 int first, int step, double rc2, double off0,
