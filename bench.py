@@ -402,9 +402,10 @@ def e2e_cold_field(case, size, axes):
     tables), then vext_field_adjoint into page-locked host memory -- region
     lists, the batch's autotuning, graph capture, pair work, results in host
     memory -- by the host clock from before the system exists.  Measured
-    twice: with the autotuner timing its candidates afresh (the cost of the
-    first field of its size class in a process), and with the pick of the
-    process-wide tuning cache (every later field of that class)."""
+    with the autotuner timing its candidates afresh (the cost of the first
+    field of its size class in a process) and with the pick of the
+    process-wide tuning cache (every later field of that class); the median
+    of three runs of each."""
     import torch
     from string_vext_b200 import _lib
     from string_vext_b200.system import VextSystem
@@ -413,21 +414,24 @@ def e2e_cold_field(case, size, axes):
     h_energy = torch.empty(shape, dtype=torch.float32, pin_memory=True)
     h_grad = torch.empty(shape + (6,), dtype=torch.float32, pin_memory=True)
     lib = _lib.load()
-    out = {}
-    for label, variant in (("tuned_afresh", 2048), ("tuning_cached", 0)):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        system = VextSystem(case)
-        opt = _lib.options(variant=variant)
-        _lib.check(lib.vext_field_adjoint(system.handle, size, n_axes, _lib.ptr(axes),
-                                          ctypes.byref(opt), _lib.ptr(h_energy),
-                                          _lib.ptr(h_grad)))
-        out[label] = time.perf_counter() - t0
-        system.close()
+    runs = {"tuned_afresh": [], "tuning_cached": []}
+    for _ in range(3):   # the median of three: device-memory set-up and release vary a lot
+        for label, variant in (("tuned_afresh", 2048), ("tuning_cached", 0)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            system = VextSystem(case)
+            opt = _lib.options(variant=variant)
+            _lib.check(lib.vext_field_adjoint(system.handle, size, n_axes, _lib.ptr(axes),
+                                              ctypes.byref(opt), _lib.ptr(h_energy),
+                                              _lib.ptr(h_grad)))
+            runs[label].append(time.perf_counter() - t0)
+            system.close()
+    out = {k: float(np.median(v)) for k, v in runs.items()}
     poses = size ** 3 * n_axes
     return {"value": poses / out["tuning_cached"], "unit": "poses/s",
             "seconds": out["tuning_cached"], "seconds_tuned_afresh": out["tuned_afresh"],
             "value_tuned_afresh": poses / out["tuned_afresh"],
+            "runs_s": {k: [round(x, 4) for x in v] for k, v in runs.items()},
             "h2d_bytes": axes.nbytes, "d2h_bytes": h_energy.numel() * 4 + h_grad.numel() * 4,
             "path": "fresh VextSystem -> vext_field_adjoint into page-locked host memory "
                     "(region lists, autotune pick, graph capture, pair work, results in host "
