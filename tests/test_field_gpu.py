@@ -175,3 +175,20 @@ def test_fp32_naive_mode_is_bounded_and_worse_than_mixed():
     err_mixed = np.abs(mixed - ref) / np.maximum(np.abs(ref), 1.0)
     assert err_naive.max() < 1e-3
     assert err_mixed.max() < 0.1 * err_naive.max()
+
+
+def test_off_center_sites_forward_field():
+    """Unequal site masses put the sites off-center (o_1 != -o_0): the
+    forward field (FP64 and mixed) against the oracle on small_field and the
+    skewed workload."""
+    for maker in (synth.small_field, synth.skewed_field):
+        case = dict(maker())
+        case["guest_mass"] = np.array([15.0, 25.0])
+        case["total_mass"] = 40.0
+        centers, axes = grid(4)
+        ref = oracle.pose_energy(case, centers, axes)
+        with VextSystem(case) as system:
+            e64 = system.field(4, axes, mode=FP64, energy=True)["energy"]
+            mixed = system.field(4, axes, mode=MIXED, energy=True)["energy"]
+        assert rel(e64, ref).max() < 1e-10
+        assert_mixed_ok(mixed, ref)

@@ -22,8 +22,11 @@ def quat_director(q):
     return np.stack([1 - 2 * (y * y + z * z), 2 * (x * y + w * z), 2 * (x * z - w * y)], 1)
 
 
-def workload(n_paths=8):
+def workload(n_paths=8, masses=None):
     cases = synth.batch_frameworks(3) + [synth.small_field()]
+    if masses is not None:   # unequal site masses: sites off-center, o_1 != -o_0
+        cases = [dict(c, guest_mass=np.asarray(masses, dtype=float),
+                      total_mass=float(sum(masses))) for c in cases]
     paths = synth.string_paths_batch(cases, n_paths=n_paths)
     # group the paths by system (the batch's layout)
     order = sorted(range(len(paths)), key=lambda p: paths[p][0])
@@ -78,9 +81,10 @@ def rel_rows(a, b, floor=1.0):
     return np.linalg.norm(a - b, axis=-1) / np.maximum(np.linalg.norm(b, axis=-1), floor)
 
 
+@pytest.mark.parametrize("masses", [None, (15.0, 25.0)])
 @pytest.mark.parametrize("mode", [_lib.VEXT_MODE_MIXED, _lib.VEXT_MODE_FP64])
-def test_pose_batch_matches_oracle_and_single_entry(mode):
-    cases, counts, centers, quats = workload()
+def test_pose_batch_matches_oracle_and_single_entry(mode, masses):
+    cases, counts, centers, quats = workload(masses=masses)
     systems = [VextSystem(c) for c in cases]
     e, gc, gq, gu = run_batch(systems, counts, centers, quats, mode)
     e_ref, gc_ref, gu_ref = oracle_refs(cases, counts, centers, quats)
