@@ -276,7 +276,8 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
                 uz[p] = y.axes[3 * o + 2];
                 acc[p][0] = acc[p][1] = 0.0;
             }
-            const NearGeom g = near_geom(cx, cy, cz, y.off0, y.off1, y.rc2);
+            const NearGeom g = near_geom(cx, cy, cz, y.off0, y.off1, y.rc2, y.floor_out2);
+            double shift_near = 0.0;
             ChunkPlan plan;
             plan.init_range(r.off, r.n_near, r.n_near);
             stage_prologue(st, plan, y.hi, y.lo, seq);
@@ -288,13 +289,15 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
                 const int s = (seq + c) % kStages;
                 near_convert<NT>(st.hib + s * kCH, st.lob + s * kCH, ed, len);
                 __syncthreads();
-                if (y.near_mode == 2) near_chunk<P, 2>(ed, std4, len, g, ux, uy, uz, acc);
-                else near_chunk<P, 1>(ed, std4, len, g, ux, uy, uz, acc);
+                if (y.near_mode == 2)
+                    near_chunk<P, 2>(ed, std4, len, g, ux, uy, uz, acc, shift_near);
+                else
+                    near_chunk<P, 1>(ed, std4, len, g, ux, uy, uz, acc, shift_near);
                 stage_next(st, plan, y.hi, y.lo, c, seq);
             }
             seq += plan.n_chunks;
 #pragma unroll
-            for (int p = 0; p < P; ++p) e[p] = acc[p][0] + acc[p][1];
+            for (int p = 0; p < P; ++p) e[p] = acc[p][0] + acc[p][1] + 2.0 * shift_near;
         }
         // ---- far pairs (packed FP32x2)
         {
@@ -803,16 +806,7 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
         y.rc2f = (float)y.rc2;
         y.off0 = sys->offsets[0];
         y.off1 = sys->offsets[1];
-        {
-            // a site lies at least |d0| - max|o| from the entry: beyond
-            // (sqrt(max floor2) + max|o|), with a relative margin far above
-            // FP64 rounding, no pair of the pose is inside a floor
-            double fl = 0.0;
-            for (int t = 0; t < sys->n_types; ++t) fl = std::max(fl, sys->h_td[4 * t + 3]);
-            const double rf = (std::sqrt(fl) + std::max(std::fabs(y.off0), std::fabs(y.off1))) *
-                                  (1.0 + 1e-9) + 1e-9;
-            y.floor_out2 = rf * rf;
-        }
+        y.floor_out2 = floor_clear_radius2(*sys);
         y.S = size;
         y.O = n_axes;
         y.axes = b->d_axes;

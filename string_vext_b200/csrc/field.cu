@@ -31,6 +31,7 @@ struct FieldArgs {
     double rc2;
     float rc2f;
     double off0, off1;
+    double floor_out2;        // |d0|^2 beyond which no site is inside a contact floor
     int S, O;
     const double *axes;       // device [O][3]
     const RegionInfo *regs;
@@ -82,8 +83,9 @@ __global__ void __launch_bounds__(CB *G, 1) field_near_kernel(FieldArgs a) {
     double cx, cy, cz;
     frac_to_cart(a.H, (gi + .5) / a.S - r.of[0], (gj + .5) / a.S - r.of[1],
                  (gk + .5) / a.S - r.of[2], cx, cy, cz);
-    const NearGeom g = near_geom(cx, cy, cz, a.off0, a.off1, a.rc2);
+    const NearGeom g = near_geom(cx, cy, cz, a.off0, a.off1, a.rc2, a.floor_out2);
     const int obase = blockIdx.y * (G * P) + og;
+    double shift_near = 0.0;
     double ux[P], uy[P], uz[P];
     double acc[P][2];
 #pragma unroll
@@ -102,7 +104,7 @@ __global__ void __launch_bounds__(CB *G, 1) field_near_kernel(FieldArgs a) {
         const int s = c % kStages;
         near_convert<NT>(st.hib + s * kCH, st.lob + s * kCH, ed, len);
         __syncthreads();
-        near_chunk<P, MODE>(ed, std4, len, g, ux, uy, uz, acc);
+        near_chunk<P, MODE>(ed, std4, len, g, ux, uy, uz, acc, shift_near);
         stage_next(st, plan, a.hi, a.lo, c, 0);
     }
     if (cvalid) {
@@ -111,7 +113,7 @@ __global__ void __launch_bounds__(CB *G, 1) field_near_kernel(FieldArgs a) {
 #pragma unroll
         for (int p = 0; p < P; ++p) {
             const int o = obase + G * p;
-            if (o < a.O) a.e64[(size_t)o * S3 + cg] = acc[p][0] + acc[p][1];
+            if (o < a.O) a.e64[(size_t)o * S3 + cg] = acc[p][0] + acc[p][1] + 2.0 * shift_near;
         }
     }
 }
@@ -604,6 +606,7 @@ static FieldArgs make_args(System *sys, const RegionSet *rs, int n_axes, const d
     a.rc2 = sys->cutoff * sys->cutoff;
     a.rc2f = (float)a.rc2;
     a.off0 = sys->offsets[0];
+    a.floor_out2 = floor_clear_radius2(*sys);
     a.off1 = sys->offsets[1];
     a.S = rs->size;
     a.O = n_axes;

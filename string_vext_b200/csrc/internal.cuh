@@ -193,6 +193,19 @@ struct Options {
 };
 Options resolve_options(const vext_options *opt);
 
+// |d0|^2 (entry - grid center) beyond which no site of a pose lies inside any
+// type's contact floor: a site is at least |d0| - max|o| from the entry, so
+// beyond sqrt(max floor2) + max|o| (with a relative margin far above FP64
+// rounding) every pair skips the floor test without changing a bit.
+inline double floor_clear_radius2(const System &sys) {
+    double fl = 0.0;
+    for (int t = 0; t < sys.n_types; ++t) fl = std::max(fl, sys.h_td[4 * t + 3]);
+    const double rf =
+        (std::sqrt(fl) + std::max(std::fabs(sys.offsets[0]), std::fabs(sys.offsets[1]))) *
+            (1.0 + 1e-9) + 1e-9;
+    return rf * rf;
+}
+
 // Directors per work item of a batch with these options (32 or 64; its
 // regions hold 512 / that many grid centers).
 int batch_item_directors(const Options &o, bool adjoint);

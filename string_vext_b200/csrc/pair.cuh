@@ -127,12 +127,15 @@ __device__ __forceinline__ NearGeom near_geom(double cx, double cy, double cz, d
 //          d0 = x - c, t = d0 . u:  q_s = |d0|^2 + o_s^2 - 2 o_s t (|d0|^2
 //          once per entry, 1 FMA per site after t); reciprocal refined
 //          by one Newton step.  MODE 2 drops the cutoff test (near pairs are never
-//          farther apart than r_split + 2 rho_site < rc, checked on the host).
+//          farther apart than r_split + 2 rho_site < rc, checked on the host)
+//          and sums the shift once per entry into shift_sum (the caller adds
+//          2 x shift_sum, both sites, to every energy); entries farther from
+//          the center than NearGeom::floor_out2 skip the contact-floor test.
 template <int P, int MODE>
 __device__ __forceinline__ void near_chunk(const double *ed, const double *std4, int len,
                                            const NearGeom &g, const double (&ux)[P],
                                            const double (&uy)[P], const double (&uz)[P],
-                                           double (&acc)[P][2]) {
+                                           double (&acc)[P][2], double &shift_sum) {
     const double2 *ed2 = reinterpret_cast<const double2 *>(ed);
     const double2 *td2 = reinterpret_cast<const double2 *>(std4);
 #pragma unroll 1
@@ -159,6 +162,20 @@ __device__ __forceinline__ void near_chunk(const double *ed, const double *std4,
             const double dx = xy.x - g.cx, dy = xy.y - g.cy, dz = zt.x - g.cz;
             const double dd = fma(dx, dx, fma(dy, dy, dz * dz));
             const double k0 = dd + g.oo0, k1 = dd + g.oo1;
+            if (MODE == 2 && dd > g.floor_out2) {   // inside the cutoff, clear of every floor
+                shift_sum += sh.x;
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    const double tt = fma(dx, ux[p], fma(dy, uy[p], dz * uz[p]));
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const double i2 = rcp64_nr<1>(fma(q ? g.m1 : g.m0, tt, q ? k1 : k0));
+                        const double i6 = i2 * i2 * i2;
+                        acc[p][q] = fma(i6, fma(cc.x, i6, -cc.y), acc[p][q]);
+                    }
+                }
+                continue;
+            }
 #pragma unroll
             for (int p = 0; p < P; ++p) {
                 const double tt = fma(dx, ux[p], fma(dy, uy[p], dz * uz[p]));
