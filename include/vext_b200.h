@@ -148,11 +148,15 @@ typedef struct {
                                 disables refinement; defaults via
                                 vext_default_options                          */
     int centers_per_region;  /* 16 or 32; 0 = default (16)                    */
-    int variant;             /* pair-kernel shape; 0 = default.  Forward +
-                                adjoint batches: bit 4096 re-evaluates poses
-                                with a shell pair within 1.25e-4 A^2 of the
-                                cutoff wholly in FP64 instead of re-testing
-                                only their shell pairs                        */
+    int variant;             /* 0 = default.  Forward + adjoint batches
+                                (studies and checks): bit 32 / 64 the
+                                reciprocal of q^3 with / without a Newton
+                                step, 128 / 512 FP32 gradient partials over
+                                16 / 64 entries, 1024 no cutoff-border test,
+                                4096 re-evaluates poses with a shell pair
+                                within 1.25e-4 A^2 of the cutoff wholly in
+                                FP64 instead of re-testing only their shell
+                                pairs; 2048 see batch_shape                   */
     int batch_shape;         /* batches: 1 + index of the CTA shape to run at
                                 full occupancy instead of autotuning; 0 =
                                 autotune (vext_batch_tuning lists the shapes);
