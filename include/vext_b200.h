@@ -156,7 +156,11 @@ typedef struct {
                                 4096 re-evaluates poses with a shell pair
                                 within 1.25e-4 A^2 of the cutoff wholly in
                                 FP64 instead of re-testing only their shell
-                                pairs; 2048 see batch_shape.  Forward field:
+                                pairs; 8192 evaluates both sites of the
+                                outer shell entries (beyond rc + the region
+                                radius, where only one site of a director
+                                can be inside); 2048 see batch_shape.
+                                Forward field:
                                 9 runs the earlier far kernel (reciprocal of
                                 q^3, every far entry masked)                  */
     int batch_shape;         /* batches: 1 + index of the CTA shape to run at

@@ -90,7 +90,7 @@ struct BatchArgs {
 // pair too close to the cutoff for the FP32 test; 2: the smallest
 // | |d0 . u| - |T*| | (symmetric sites), 2 |o| times which is the former.
 template <int CB, int G, int P, bool NEWTON, bool RCP1, int UNROLL, int FLUSH, bool GSUM,
-          int BORDER>
+          int BORDER, bool OUTER>
 __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSys &y,
                                                const RegionInfo &r, Stager &st, double *ed,
                                                const float4 *stf, const double *std4,
@@ -170,11 +170,19 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
             uz[j] = make_float2((float)y.axes[3 * o0 + 2], (float)y.axes[3 * o1 + 2]);
         }
         const FarGeom g = far_geom(cx, cy, cz, y.off0, y.off1, y.rc2f);
+        // inner entries, the shell, then (symmetric sites) the outer shell,
+        // where only the near site of each director can be inside
+        const int n_outer = SYM && OUTER ? r.n_outer : 0;
 #pragma unroll 1
-        for (int pass = 0; pass < 2; ++pass) {   // inner entries, then the shell
+        for (int pass = 0; pass < 3; ++pass) {
             ChunkPlan plan;
-            plan.init_range(r.off + r.n_near + (pass ? r.n_inner : 0), 0,
-                            pass ? r.n_total - r.n_near - r.n_inner : r.n_inner);
+            if (pass == 0)
+                plan.init_range(r.off + r.n_near, 0, r.n_inner);
+            else if (pass == 1)
+                plan.init_range(r.off + r.n_near + r.n_inner, 0,
+                                r.n_total - r.n_near - r.n_inner - n_outer);
+            else
+                plan.init_range(r.off + r.n_total - n_outer, 0, n_outer);
             stage_prologue(st, plan, y.hi, y.lo, seq);
             for (int c = 0; c < plan.n_chunks; ++c) {
                 if (!stage_wait(st, plan, c, seq, a.status)) return false;
@@ -183,12 +191,17 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
                 plan.chunk(c, start, len, near);
                 const float4 *hb = st.hib + ((seq + c) % kStages) * kCH;
                 constexpr int GNT = GSUM ? NT : 0;
-                if (pass)
+                if (pass == 2) {
+                    if constexpr (SYM && OUTER)
+                        far_chunk_outer<P, FLUSH, UNROLL, GNT, BORDER>(hb, stf, len, g, ux, uy,
+                                                                       uz, acc, gsum, border);
+                } else if (pass == 1) {
                     far_chunk_adj<P, NEWTON, FLUSH, true, RCP1, UNROLL, GNT, BORDER, SYM>(
                         hb, stf, len, g, ux, uy, uz, acc, shift_sum, gsum, border);
-                else
+                } else {
                     far_chunk_adj<P, NEWTON, FLUSH, false, RCP1, UNROLL, GNT, 0, SYM>(
                         hb, stf, len, g, ux, uy, uz, acc, shift_sum, gsum);
+                }
                 stage_next(st, plan, y.hi, y.lo, c, seq);
             }
             seq += plan.n_chunks;
@@ -212,10 +225,11 @@ __device__ __forceinline__ bool batch_item_adj(const BatchArgs &a, const BatchSy
 // 128-entry chunk; 8 = as 1 with the FP64 gradient sums in shared memory
 // during the far passes (fewer registers: more resident CTAs); 11 / 12 = as
 // 8 / 1 with the far entry loop unrolled twice; 17 = as 8 unrolled four
-// times.  BORDER: 0 none, 1 the
+// times.  OUTER (symmetric sites, BORDER 2): the outer shell entries in the
+// single-site pass (far_chunk_outer).  BORDER: 0 none, 1 the
 // cutoff-border test per site (|q - rc^2|), 2 per director (| |d0 . u| -
 // |T*| |, symmetric sites only).
-template <int CB, int G, int P, int MINB, int ADJ, int BORDER = 0>
+template <int CB, int G, int P, int MINB, int ADJ, int BORDER = 0, bool OUTER = false>
 __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
     constexpr int NT = CB * G, PP = P / 2;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -261,7 +275,7 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
         if constexpr (ADJ) {
             double *gsum = reinterpret_cast<double *>(std4 + 4 * y.n_types);
             if (!batch_item_adj<CB, G, P, ADJ == 2, ADJ == 1 || ADJ >= 5, kUnroll,
-                                ADJ == 6 ? 16 : ADJ == 7 ? 64 : 128, kGsum, BORDER>(
+                                ADJ == 6 ? 16 : ADJ == 7 ? 64 : 128, kGsum, BORDER, OUTER>(
                     a, y, r, st, ed, stf, std4, gsum, seq, cx, cy, cz, obase, e, gr, border))
                 return;
         } else {
@@ -314,11 +328,19 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
             }
             const FarGeom g = far_geom(cx, cy, cz, y.off0, y.off1, y.rc2f);
             double shift_sum = 0.0;
+            // inner entries, the shell, then (symmetric sites) the outer
+            // shell, where only the near site of each director can be inside
+            const int n_outer = y.off0 != 0.0 && y.off1 == -y.off0 ? r.n_outer : 0;
 #pragma unroll 1
-            for (int pass = 0; pass < 2; ++pass) {   // inner entries, then the shell
+            for (int pass = 0; pass < 3; ++pass) {
                 ChunkPlan plan;
-                plan.init_range(r.off + r.n_near + (pass ? r.n_inner : 0), 0,
-                                pass ? r.n_total - r.n_near - r.n_inner : r.n_inner);
+                if (pass == 0)
+                    plan.init_range(r.off + r.n_near, 0, r.n_inner);
+                else if (pass == 1)
+                    plan.init_range(r.off + r.n_near + r.n_inner, 0,
+                                    r.n_total - r.n_near - r.n_inner - n_outer);
+                else
+                    plan.init_range(r.off + r.n_total - n_outer, 0, n_outer);
                 stage_prologue(st, plan, y.hi, y.lo, seq);
                 for (int c = 0; c < plan.n_chunks; ++c) {
                     if (!stage_wait(st, plan, c, seq, a.status)) return;
@@ -326,7 +348,8 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
                     bool near;
                     plan.chunk(c, start, len, near);
                     const float4 *hb = st.hib + ((seq + c) % kStages) * kCH;
-                    if (pass) far_chunk_fwd<P, 16, true>(hb, stf, len, g, ux, uy, uz, acc, shift_sum);
+                    if (pass == 2) far_chunk_fwd_outer<P, 16>(hb, stf, len, g, ux, uy, uz, acc);
+                    else if (pass) far_chunk_fwd<P, 16, true>(hb, stf, len, g, ux, uy, uz, acc, shift_sum);
                     else far_chunk_fwd<P, 16, false>(hb, stf, len, g, ux, uy, uz, acc, shift_sum);
                     stage_next(st, plan, y.hi, y.lo, c, seq);
                 }
@@ -541,13 +564,18 @@ static const BatchKernel kAdjointFlush64Kernels[] = {   // accuracy/speed study
 static const BatchKernel kForwardCb8Kernels[] = {
     {batch_field_kernel<8, 16, 4, 4, 0>, 128, "8c 128x4"},
     {batch_field_kernel<8, 32, 2, 3, 0>, 256, "8c 256x2"}};
-static const BatchKernel kAdjointCb8Kernels[] = {   // symmetric sites: border per director
-    {batch_field_kernel<8, 16, 4, 3, 8, 2>, 128, "8c 128x4/3 gsum"},
-    {batch_field_kernel<8, 16, 4, 2, 1, 2>, 128, "8c 128x4"},
-    {batch_field_kernel<8, 32, 2, 2, 1, 2>, 256, "8c 256x2"},
-    {batch_field_kernel<8, 16, 4, 3, 11, 2>, 128, "8c 128x4/3 gsum unroll2"},
-    {batch_field_kernel<8, 16, 4, 2, 12, 2>, 128, "8c 128x4 unroll2"},
-    {batch_field_kernel<8, 16, 4, 3, 17, 2>, 128, "8c 128x4/3 gsum unroll4"}};
+// symmetric sites: border per director, outer shell in the single-site pass
+static const BatchKernel kAdjointCb8Kernels[] = {
+    {batch_field_kernel<8, 16, 4, 3, 8, 2, true>, 128, "8c 128x4/3 gsum"},
+    {batch_field_kernel<8, 16, 4, 2, 1, 2, true>, 128, "8c 128x4"},
+    {batch_field_kernel<8, 32, 2, 2, 1, 2, true>, 256, "8c 256x2"},
+    {batch_field_kernel<8, 16, 4, 3, 11, 2, true>, 128, "8c 128x4/3 gsum unroll2"},
+    {batch_field_kernel<8, 16, 4, 2, 12, 2, true>, 128, "8c 128x4 unroll2"},
+    {batch_field_kernel<8, 16, 4, 3, 17, 2, true>, 128, "8c 128x4/3 gsum unroll4"}};
+// the same with the outer shell in the two-site shell pass (timing study)
+static const BatchKernel kAdjointCb8TwoSiteKernels[] = {
+    {batch_field_kernel<8, 16, 4, 3, 11, 2>, 128, "8c 128x4/3 gsum unroll2, two-site outer"},
+    {batch_field_kernel<8, 16, 4, 3, 17, 2>, 128, "8c 128x4/3 gsum unroll4, two-site outer"}};
 static const BatchKernel kAdjointCb8SiteBorderKernels[] = {   // any sites: border per site
     {batch_field_kernel<8, 16, 4, 3, 8, 1>, 128, "8c 128x4/3 gsum, border/site"},
     {batch_field_kernel<8, 16, 4, 2, 1, 1>, 128, "8c 128x4, border/site"},
@@ -570,7 +598,8 @@ constexpr int kMaxCandidates = 12;
 // 128-entry chunk by default; the energy partials always cover 16), 6 default
 // on 8-center regions with 64-director items, 7 forward on 8-center regions,
 // 8 as 6 without the cutoff-border test, 9 as 6 with the border test per site
-// (guests whose sites are not symmetric about the center)
+// (guests whose sites are not symmetric about the center), 10 as 6 with the
+// outer shell in the two-site shell pass
 static int batch_kernel_count(int kind) {
     switch (kind) {
     case 0: return VEXT_COUNT(kForwardKernels);
@@ -582,6 +611,7 @@ static int batch_kernel_count(int kind) {
     case 7: return VEXT_COUNT(kForwardCb8Kernels);
     case 8: return VEXT_COUNT(kAdjointCb8NoBorderKernels);
     case 9: return VEXT_COUNT(kAdjointCb8SiteBorderKernels);
+    case 10: return VEXT_COUNT(kAdjointCb8TwoSiteKernels);
     default: return VEXT_COUNT(kAdjointRcp3Kernels);
     }
 }
@@ -597,6 +627,7 @@ static const BatchKernel &batch_kernel(int kind, int shape) {
     case 7: return kForwardCb8Kernels[shape];
     case 8: return kAdjointCb8NoBorderKernels[shape];
     case 9: return kAdjointCb8SiteBorderKernels[shape];
+    case 10: return kAdjointCb8TwoSiteKernels[shape];
     default: return kAdjointRcp3Kernels[shape];
     }
 }
@@ -613,12 +644,13 @@ static int batch_kind(const Options &o, bool adj) {
     if (o.variant & 128) return 4;
     if (o.variant & 512) return 5;
     if (o.variant & 1024) return cb16 ? 1 : 8;
+    if (o.variant & 8192) return cb16 ? 1 : 10;
     return cb16 ? 1 : 6;
 }
 
 int batch_item_directors(const Options &o, bool adj) {
     const int kind = batch_kind(o, adj);
-    return kind >= 6 && kind <= 9 ? 64 : 32;
+    return kind >= 6 && kind <= 10 ? 64 : 32;
 }
 
 }  // namespace vext
@@ -865,11 +897,12 @@ int batch_build(int n_systems, const vext_system *systems, int size, int n_axes,
     const int size_class =
         (int)std::lround(std::log2(std::max(mean_len, 1.0))) * 64 +
         (int)std::lround(std::log2((double)std::max<size_t>(items.size(), 1)));
-    // kind 6 (the per-director border test, q_1 from the site-0 terms)
-    // assumes exactly symmetric sites, o_1 = -o_0 != 0 (two identical sites
+    // kinds 6 and 10 (the per-director border test, q_1 from the site-0
+    // terms, the single-site outer shell pass of kind 6) assume exactly
+    // symmetric sites, o_1 = -o_0 != 0 (two identical sites
     // about their center of mass); other guests take the same shapes with the
     // per-site test and both sites' terms
-    if (b->kind == 6)
+    if (b->kind == 6 || b->kind == 10)
         for (const BatchSys &y : hs)
             if (y.off0 == 0.0 || y.off1 != -y.off0) b->kind = 9;
     for (const BatchSys &y : hs) b->targets.push_back({y.out, y.grad});

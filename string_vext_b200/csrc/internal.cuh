@@ -13,7 +13,9 @@
 //                            relative position to ~1e-14 A
 // Each region's entries are contiguous (info.off), "near" entries first:
 // entries closer to the origin than r_split + max|offset| + rho are near,
-// so every (site, image) pair nearer than r_split has a near entry.
+// so every (site, image) pair nearer than r_split has a near entry.  Then
+// the far inner entries, then the shell, whose last n_outer entries lie
+// beyond rc + rho + 1e-3 A of the origin.
 #pragma once
 
 #include <mutex>
@@ -36,7 +38,8 @@ struct alignas(16) RegionInfo {
     int ni, nj, nk;     // grid centers per axis (field regions)
     int n_inner;        // far entries within the cutoff of every site of every pose of the
                         // region (they follow the near entries; the shell ones come last)
-    int pad;
+    int n_outer;        // the last shell entries: beyond rc + rho + 1e-3 A of the origin,
+                        // hence beyond rc of every pose center of the region
 };
 static_assert(sizeof(RegionInfo) % 16 == 0, "RegionInfo must stay 16-byte aligned");
 

@@ -558,6 +558,67 @@ __device__ __forceinline__ void far_chunk_fwd(const float4 *hb, const float4 *st
     }
 }
 
+// Forward far chunk over outer shell entries (RegionInfo::n_outer: |d0| >
+// rc for every pose center of the region), symmetric sites (o_1 = -o_0):
+// only a director's site on the entry's side can be inside the cutoff, q =
+// |d0|^2 + o^2 - |2 o t|, so only that one is evaluated (masked as in
+// far_chunk_fwd); the other adds exactly nothing there too.  (The batched
+// forward kernel takes it; in the per-field far kernel, bounded to 80
+// registers, the third pass cost spills and more time than it saved.)
+template <int P, int FLUSH, int UNROLL = 2>
+__device__ __forceinline__ void far_chunk_fwd_outer(const float4 *hb, const float4 *stf, int len,
+                                                    const FarGeom &g, const float2 (&ux)[P / 2],
+                                                    const float2 (&uy)[P / 2],
+                                                    const float2 (&uz)[P / 2],
+                                                    double (&acc)[P]) {
+    constexpr int PP = P / 2;
+    const float2 nam = make_float2(-fabsf(g.m0.x), -fabsf(g.m0.x));   // -|m0|
+#pragma unroll 1
+    for (int e0 = 0; e0 < len; e0 += FLUSH) {
+        float2 fa[PP];
+#pragma unroll
+        for (int j = 0; j < PP; ++j) fa[j] = make_float2(0.f, 0.f);
+        const int e1 = min(e0 + FLUSH, len);
+#pragma unroll UNROLL
+        for (int e = e0; e < e1; ++e) {
+            float2 k0, dx2, dy2, dz2, c12, mc6, sh;
+            {
+                const float4 h = hb[e];
+                const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, -)
+                const float dx = h.x - g.cx, dy = h.y - g.cy, dz = h.z - g.cz;
+                const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                if (dd > g.out2) continue;
+                k0 = make_float2(dd + g.oo0, dd + g.oo0);
+                dx2 = make_float2(dx, dx);
+                dy2 = make_float2(dy, dy);
+                dz2 = make_float2(dz, dz);
+                c12 = make_float2(tp.x, tp.x);
+                mc6 = make_float2(-tp.y, -tp.y);
+                sh = make_float2(tp.z, tp.z);
+            }
+#pragma unroll
+            for (int j = 0; j < PP; ++j) {
+                const float2 t =
+                    __ffma2_rn(dx2, ux[j], __ffma2_rn(dy2, uy[j], __fmul2_rn(dz2, uz[j])));
+                const float2 d2 = __ffma2_rn(nam, make_float2(fabsf(t.x), fabsf(t.y)), k0);
+                float r0, r1;
+                asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(d2.x));
+                asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r1) : "f"(d2.y));
+                const float2 n1 = make_float2(r0, r1);
+                const float2 m = make_float2(set_lt(d2.x, g.rc2f), set_lt(d2.y, g.rc2f));
+                const float2 n3 = __fmul2_rn(__fmul2_rn(__fmul2_rn(n1, n1), n1), m);
+                fa[j] = __ffma2_rn(m, sh, fa[j]);
+                fa[j] = __ffma2_rn(n3, __ffma2_rn(c12, n3, mc6), fa[j]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < PP; ++j) {
+            acc[2 * j] += (double)fa[j].x;
+            acc[2 * j + 1] += (double)fa[j].y;
+        }
+    }
+}
+
 // ------------------------------------------------------------ adjoint
 //
 // Forward + adjoint sums of one pose (center c, unit director u, sites at
@@ -894,6 +955,130 @@ __device__ __forceinline__ void far_chunk_adj(const float4 *hb, const float4 *st
                 }
             }
         }
+    }
+}
+
+// Outer shell entries (RegionInfo::n_outer: beyond rc + rho + 1e-3 A of the
+// region origin, so |d0| > rc for every pose center of the region), symmetric
+// sites only.  With q_s = k0 + m_s t and m_1 = -m_0, a director's site on the
+// entry's side (m_s t <= 0) has q = k0 - |m_0| |t| and the other q >= k0 =
+// |d0|^2 + o^2 > rc^2: at most the near one is inside.  Only that one is
+// evaluated, with the operations of far_chunk_adj (fma(-|m0|, |t|, k0) is
+// the near site's fma(m_s, t, k0) bit for bit); the other is out in FP32
+// (its q is at least k0, which exceeds rc^2 by 0.025 A^2 and more) as in
+// FP64, so shell_border_repair sees the decisions this loop took.  Gradient
+// partials: A = sum fp d0, B = sum sigma fp d0, C = sum sigma fp (sigma = +1
+// where the near site is site 0, -1 where it is site 1), flushed as H_0 =
+// (A + B) / 2, H_1 = (A - B) / 2 and F_0 - F_1 = C (f[0] of the symmetric
+// loops).  BORDER 2: the per-director cutoff-border test of far_chunk_adj.
+template <int P, int FLUSH, int UNROLL, int GSUM_NT, int BORDER>
+__device__ __forceinline__ void far_chunk_outer(const float4 *hb, const float4 *stf, int len,
+                                                const FarGeom &g, const float2 (&ux)[P / 2],
+                                                const float2 (&uy)[P / 2],
+                                                const float2 (&uz)[P / 2], AdjAcc (&acc)[P],
+                                                double *gsum = nullptr,
+                                                float *border = nullptr) {
+    static_assert(BORDER != 1, "the outer loop serves the symmetric-site kernels");
+    constexpr int PP = P / 2;
+    const float2 nam = make_float2(-fabsf(g.m0.x), -fabsf(g.m0.x));   // -|m0|
+    const bool m0neg = g.m0.x < 0.f;   // site 0 is the near one where t > 0
+#pragma unroll 1
+    for (int e0 = 0; e0 < len; e0 += FLUSH) {
+        float2 fa[PP][3], fb[PP][3], fc[PP];
+#pragma unroll
+        for (int j = 0; j < PP; ++j) {
+            fc[j] = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) fa[j][k] = fb[j][k] = make_float2(0.f, 0.f);
+        }
+        const int e1 = min(e0 + FLUSH, len);
+#pragma unroll 1
+        for (int b0 = e0; b0 < e1; b0 += 16) {   // energy partials: 16 entries
+            float2 fe[PP];
+#pragma unroll
+            for (int j = 0; j < PP; ++j) fe[j] = make_float2(0.f, 0.f);
+            const int b1 = min(b0 + 16, e1);
+#pragma unroll UNROLL
+            for (int e = b0; e < b1; ++e) {
+                float2 k0, dx2, dy2, dz2, c12, c6, sh, mc6, m2c12;
+                float ts = 0.f;
+                {
+                    const float4 h = hb[e];
+                    const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, -)
+                    const float dx = h.x - g.cx, dy = h.y - g.cy, dz = h.z - g.cz;
+                    const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    if (dd > g.out2) continue;
+                    k0 = make_float2(dd + g.oo0, dd + g.oo0);
+                    dx2 = make_float2(dx, dx);
+                    dy2 = make_float2(dy, dy);
+                    dz2 = make_float2(dz, dz);
+                    c12 = make_float2(tp.x, tp.x);
+                    c6 = make_float2(tp.y, tp.y);
+                    sh = make_float2(tp.z, tp.z);
+                    mc6 = make_float2(-tp.y, -tp.y);
+                    m2c12 = make_float2(-2.f * tp.x, -2.f * tp.x);
+                    if (BORDER == 2) ts = fabsf(fmaf(dd, g.inv2o, g.tb));
+                }
+#pragma unroll
+                for (int j = 0; j < PP; ++j) {
+                    const float2 t =
+                        __ffma2_rn(dx2, ux[j], __ffma2_rn(dy2, uy[j], __fmul2_rn(dz2, uz[j])));
+                    const float2 at = make_float2(fabsf(t.x), fabsf(t.y));
+                    if (BORDER == 2) {
+                        border[2 * j] = fminf(border[2 * j], fabsf(at.x - ts));
+                        border[2 * j + 1] = fminf(border[2 * j + 1], fabsf(at.y - ts));
+                    }
+                    const float2 d2 = __ffma2_rn(nam, at, k0);
+                    float r0, r1;
+                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(d2.x));
+                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r1) : "f"(d2.y));
+                    const float2 n1 = make_float2(r0, r1);
+                    float2 n3 = __fmul2_rn(__fmul2_rn(n1, n1), n1);
+                    const float2 m = make_float2(set_lt(d2.x, g.rc2f), set_lt(d2.y, g.rc2f));
+                    n3 = __fmul2_rn(n3, m);
+                    fe[j] = __ffma2_rn(m, sh, fe[j]);
+                    fe[j] = __ffma2_rn(n3, __ffma2_rn(c12, n3, mc6), fe[j]);
+                    const float2 fp = __fmul2_rn(__fmul2_rn(n1, n3), __ffma2_rn(m2c12, n3, c6));
+                    const float2 sfp = make_float2((t.x > 0.f) == m0neg ? fp.x : -fp.x,
+                                                   (t.y > 0.f) == m0neg ? fp.y : -fp.y);
+                    fa[j][0] = __ffma2_rn(fp, dx2, fa[j][0]);
+                    fa[j][1] = __ffma2_rn(fp, dy2, fa[j][1]);
+                    fa[j][2] = __ffma2_rn(fp, dz2, fa[j][2]);
+                    fb[j][0] = __ffma2_rn(sfp, dx2, fb[j][0]);
+                    fb[j][1] = __ffma2_rn(sfp, dy2, fb[j][1]);
+                    fb[j][2] = __ffma2_rn(sfp, dz2, fb[j][2]);
+                    fc[j] = __fadd2_rn(sfp, fc[j]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < PP; ++j) {
+                acc[2 * j].e += (double)fe[j].x;
+                acc[2 * j + 1].e += (double)fe[j].y;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < PP; ++j)
+#pragma unroll
+            for (int l = 0; l < 2; ++l) {
+                const int p = 2 * j + l;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const double a = (double)(l ? fa[j][k].y : fa[j][k].x);
+                    const double b = (double)(l ? fb[j][k].y : fb[j][k].x);
+                    if constexpr (GSUM_NT > 0) {
+                        grad_slot<GSUM_NT>(gsum, p, k) += 0.5 * (a + b);
+                        grad_slot<GSUM_NT>(gsum, p, 3 + k) += 0.5 * (a - b);
+                    } else {
+                        acc[p].h[0][k] += 0.5 * (a + b);
+                        acc[p].h[1][k] += 0.5 * (a - b);
+                    }
+                }
+                const double c = (double)(l ? fc[j].y : fc[j].x);
+                if constexpr (GSUM_NT > 0)
+                    grad_slot<GSUM_NT>(gsum, p, 6) += c;
+                else
+                    acc[p].f[0] += c;
+            }
     }
 }
 

@@ -107,6 +107,7 @@ struct BuildArgs {
     double r_list0;   // rc + max|offset| (+ margin)
     double r_near0;   // r_split + max|offset| (+ margin)
     double r_inner0;  // cutoff - max|offset| (- margin): inner entries lie within r_inner0 - rho
+    double r_outer0;  // cutoff + 1e-3 A: outer shell entries lie beyond r_outer0 + rho
 };
 
 // Visit every candidate image of atom j for a region; f(dist2, rel) per image.
@@ -188,21 +189,24 @@ __global__ void __launch_bounds__(kBuildThreads)
     const RegionInfo r = regs[region];
     const double rl = a.r_list0 + r.rho, rn = a.r_near0 + r.rho, rn2 = rn * rn;
     const double ri = a.r_inner0 - r.rho, ri2 = ri > 0 ? ri * ri : 0.0;
-    int near = 0, inner = 0, total = 0;
+    const double ro = a.r_outer0 + r.rho, ro2 = ro * ro;
+    int near = 0, inner = 0, outer = 0, total = 0;
     for (int j = threadIdx.x; j < a.n_atoms; j += kBuildThreads)
         for_each_image(a, r, j, rl, [&](double q, double, double, double) {
             ++total;
             near += q < rn2;
             inner += q >= rn2 && q < ri2;
+            outer += q >= rn2 && q >= ri2 && q >= ro2;
         });
     __shared__ int sh[128];
     int pa, pb, ta, tb, pc, pd, tc, td;
     block_scan2<kBuildThreads>(near, total, pa, pb, ta, tb, sh);
-    block_scan2<kBuildThreads>(inner, 0, pc, pd, tc, td, sh);
+    block_scan2<kBuildThreads>(inner, outer, pc, pd, tc, td, sh);
     if (threadIdx.x == 0) {
         regs[region].n_near = ta;
         regs[region].n_total = tb;
         regs[region].n_inner = tc;
+        regs[region].n_outer = td;
     }
 }
 
@@ -214,28 +218,36 @@ __global__ void __launch_bounds__(kBuildThreads)
     const RegionInfo r = regs[region];
     const double rl = a.r_list0 + r.rho, rn = a.r_near0 + r.rho, rn2 = rn * rn;
     const double ri = a.r_inner0 - r.rho, ri2 = ri > 0 ? ri * ri : 0.0;
+    const double ro = a.r_outer0 + r.rho, ro2 = ro * ro;
     __shared__ int sh[128];
-    // entry order: near | far inner | far shell, atom-major inside each class
-    int base_near = 0, base_inner = r.n_near, base_shell = r.n_near + r.n_inner;
+    // entry order: near | far inner | far shell | outer shell, atom-major
+    // inside each class
+    const int end_shell = r.n_total - r.n_outer;
+    int base_near = 0, base_inner = r.n_near, base_shell = r.n_near + r.n_inner,
+        base_outer = end_shell;
     for (int j0 = 0; j0 < a.n_atoms; j0 += kBuildThreads) {
         const int j = j0 + threadIdx.x;
-        int near = 0, inner = 0, shell = 0;
+        int near = 0, inner = 0, shell = 0, outer = 0;
         if (j < a.n_atoms)
             for_each_image(a, r, j, rl, [&](double q, double, double, double) {
                 if (q < rn2) ++near;
                 else if (q < ri2) ++inner;
-                else ++shell;
+                else if (q < ro2) ++shell;
+                else ++outer;
             });
-        int pn, pi, tn, ti, ps, pz, ts, tz;
+        int pn, pi, tn, ti, ps, po, ts, to;
         block_scan2<kBuildThreads>(near, inner, pn, pi, tn, ti, sh);
-        block_scan2<kBuildThreads>(shell, 0, ps, pz, ts, tz, sh);
+        block_scan2<kBuildThreads>(shell, outer, ps, po, ts, to, sh);
         if (j < a.n_atoms) {
-            int wn = base_near + pn, wi = base_inner + pi, ws = base_shell + ps;
+            int wn = base_near + pn, wi = base_inner + pi, ws = base_shell + ps,
+                wo = base_outer + po;
             const int t = a.type[j];
             for_each_image(a, r, j, rl, [&](double q, double x, double y, double z) {
-                const int cls = q < rn2 ? 0 : (q < ri2 ? 1 : 2);
-                const int slot = cls == 0 ? wn++ : (cls == 1 ? wi++ : ws++);
-                const int end = cls == 0 ? r.n_near : (cls == 1 ? r.n_near + r.n_inner : r.n_total);
+                const int cls = q < rn2 ? 0 : (q < ri2 ? 1 : (q < ro2 ? 2 : 3));
+                const int slot = cls == 0 ? wn++ : (cls == 1 ? wi++ : (cls == 2 ? ws++ : wo++));
+                const int end = cls == 0 ? r.n_near
+                                         : (cls == 1 ? r.n_near + r.n_inner
+                                                     : (cls == 2 ? end_shell : r.n_total));
                 if (slot >= end) {
                     atomicExch(status, DEV_BAD_LIST);
                     return;
@@ -248,9 +260,10 @@ __global__ void __launch_bounds__(kBuildThreads)
         base_near += tn;
         base_inner += ti;
         base_shell += ts;
+        base_outer += to;
     }
     if (threadIdx.x == 0 && (base_near != r.n_near || base_inner != r.n_near + r.n_inner ||
-                             base_shell != r.n_total))
+                             base_shell != end_shell || base_outer != r.n_total))
         atomicExch(status, DEV_BAD_LIST);
 }
 
@@ -274,6 +287,7 @@ static int build_lists(System *sys, RegionSet *rs, cudaStream_t stream) {
     a.r_list0 = sys->cutoff + sys->max_offset + 1e-6;
     a.r_near0 = rs->r_split + sys->max_offset + 1e-6;
     a.r_inner0 = sys->cutoff - sys->max_offset - 1e-6;
+    a.r_outer0 = sys->cutoff + 1e-3;
     const int n = rs->n_regions;
     if (!rs->d_info) VEXT_CUDA(cudaMalloc(&rs->d_info, sizeof(RegionInfo) * n));
     VEXT_CUDA(cudaMemcpyAsync(rs->d_info, rs->h_info.data(), sizeof(RegionInfo) * n,
@@ -320,7 +334,7 @@ int get_field_regions(System *sys, int size, int cb, double r_split, RegionSet *
     for (RegionSet *rs : sys->sets)
         if (rs->size == size && rs->bi * rs->bj * rs->bk == cb && rs->r_split == r_split) {
             if (rs->stale) {
-                for (auto &r : rs->h_info) r.n_near = r.n_total = r.n_inner = 0;
+                for (auto &r : rs->h_info) r.n_near = r.n_total = r.n_inner = r.n_outer = 0;
                 VEXT_TRY(build_lists(sys, rs, stream));
             }
             *out = rs;
@@ -370,7 +384,7 @@ int get_bin_regions(System *sys, double r_split, RegionSet **out, cudaStream_t s
     for (RegionSet *rs : sys->sets)
         if (rs->size == 0 && rs->r_split == r_split && rs->bin_width == bin_width) {
             if (rs->stale) {
-                for (auto &r : rs->h_info) r.n_near = r.n_total = r.n_inner = 0;
+                for (auto &r : rs->h_info) r.n_near = r.n_total = r.n_inner = r.n_outer = 0;
                 VEXT_TRY(build_lists(sys, rs, stream));
             }
             *out = rs;

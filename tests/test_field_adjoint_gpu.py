@@ -462,3 +462,47 @@ def test_asymmetric_guest_takes_the_per_site_kernels():
         gm = grad.cpu().numpy().astype(np.float64)
         grel = np.linalg.norm(gm - gx, axis=-1) / np.maximum(np.linalg.norm(gx, axis=-1), 1.0)
         assert grel.max() < 1e-5
+
+
+def test_outer_shell_single_site_pass_matches_two_site_pass():
+    """Outer shell entries (beyond rc + the region radius from the region
+    origin) can have only a director's site on their side inside the cutoff,
+    so the default symmetric-site kernels evaluate that site alone there.
+    Variant 8192 evaluates both sites as in the rest of the shell: the two
+    flag the same border poses and agree within the FP32 summation order
+    (energy at float32 storage, gradient 1e-6 relative), and both sit within
+    the bar of the plain FP64 adjoint."""
+    for case in (synth.small_field(), synth.batch_frameworks(1)[0]):
+        size = 12
+        _, axes = regular_pose_grid(size, 64)
+        axes = normalized_directors(axes)
+        shape = (64, size, size, size)
+        with VextSystem(case) as system:
+            res = {}
+            for variant in (0, 8192):
+                out = torch.empty(shape, dtype=torch.float32, device="cuda")
+                grad = torch.empty(shape + (6,), dtype=torch.float32, device="cuda")
+                batch = VextBatch([system], size, axes, [out], gradients=[grad],
+                                  variant=variant)
+                name = batch.info()["cta_shape"]
+                assert ("two-site outer" in name) == (variant == 8192)
+                batch.run()
+                batch.check()
+                res[variant] = (batch.refined(), out.cpu().numpy().astype(np.float64),
+                                grad.cpu().numpy().astype(np.float64))
+                batch.close()
+            e64 = torch.empty(shape, dtype=torch.float64, device="cuda")
+            g64 = torch.empty(shape + (6,), dtype=torch.float64, device="cuda")
+            system.field_adjoint_device(size, axes, None, None, e64, g64,
+                                        mode=_lib.VEXT_MODE_FP64_PLAIN)
+            torch.cuda.synchronize()
+        ex, gx = e64.cpu().numpy(), g64.cpu().numpy()
+        (n1, e1, g1), (n2, e2, g2) = res[0], res[8192]
+        assert n1 == n2
+        assert (np.abs(e1 - e2) <= 2e-4 + 2.4e-7 * np.abs(e2)).all()
+        rel = np.linalg.norm(g1 - g2, axis=-1) / np.maximum(np.linalg.norm(g2, axis=-1), 1.0)
+        assert rel.max() < 1e-6
+        for e, g in ((e1, g1), (e2, g2)):
+            assert (np.abs(e - ex) <= 1e-4 + 1.2e-7 * np.abs(ex)).all()
+            grel = np.linalg.norm(g - gx, axis=-1) / np.maximum(np.linalg.norm(gx, axis=-1), 1.0)
+            assert grel.max() < 1e-5
