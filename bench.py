@@ -50,10 +50,10 @@ FLOP_FWD_ADJ = 28      # forward + adjoint
 METRIC = "Vext pose evals/s at <=1e-4 K vs FP64, fwd+adjoint evals/s; % FP32 peak"
 # dram__bytes_read.sum + dram__bytes_write.sum of one field_far2_kernel launch on
 # full_field, from an ncu capture (--set full) of `bench.py --profile field`.
-FAR_DRAM_BYTES_FULL_FIELD = 744_213_504 + 100_719_360
+FAR_DRAM_BYTES_FULL_FIELD = 776_213_504 + 100_771_584
 # the same for one forward + adjoint batch_field_kernel launch on full_field,
 # from an ncu capture (--set full) of `bench.py --profile adjoint`.
-ADJ_DRAM_BYTES_FULL_FIELD = 770_997_760 + 366_555_904
+ADJ_DRAM_BYTES_FULL_FIELD = 771_922_688 + 367_529_216
 CPU_CENTERS_PER_CORE_S = 900.0   # reference driver throughput estimate used to size the sample
 
 
