@@ -159,7 +159,9 @@ typedef struct {
                                 pairs; 8192 evaluates both sites of the
                                 outer shell entries (beyond rc + the region
                                 radius, where only one site of a director
-                                can be inside); 2048 see batch_shape.
+                                can be inside; the sums then differ only
+                                in FP32 rounding);
+                                2048 see batch_shape.
                                 Forward field:
                                 9 runs the earlier far kernel (reciprocal of
                                 q^3, every far entry masked)                  */

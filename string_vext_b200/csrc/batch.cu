@@ -328,19 +328,16 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
             }
             const FarGeom g = far_geom(cx, cy, cz, y.off0, y.off1, y.rc2f);
             double shift_sum = 0.0;
-            // inner entries, the shell, then (symmetric sites) the outer
-            // shell, where only the near site of each director can be inside
-            const int n_outer = y.off0 != 0.0 && y.off1 == -y.off0 ? r.n_outer : 0;
+            // inner entries, then the shell, whose outer entries (symmetric
+            // sites) take the near site of each director alone
+            const int shell_n = r.n_total - r.n_near - r.n_inner;
+            const bool sym = y.off0 != 0.0 && y.off1 == -y.off0;
+            const int outer_at = shell_n - (sym ? r.n_outer : 0);
 #pragma unroll 1
-            for (int pass = 0; pass < 3; ++pass) {
+            for (int pass = 0; pass < 2; ++pass) {
                 ChunkPlan plan;
-                if (pass == 0)
-                    plan.init_range(r.off + r.n_near, 0, r.n_inner);
-                else if (pass == 1)
-                    plan.init_range(r.off + r.n_near + r.n_inner, 0,
-                                    r.n_total - r.n_near - r.n_inner - n_outer);
-                else
-                    plan.init_range(r.off + r.n_total - n_outer, 0, n_outer);
+                plan.init_range(r.off + r.n_near + (pass ? r.n_inner : 0), 0,
+                                pass ? shell_n : r.n_inner);
                 stage_prologue(st, plan, y.hi, y.lo, seq);
                 for (int c = 0; c < plan.n_chunks; ++c) {
                     if (!stage_wait(st, plan, c, seq, a.status)) return;
@@ -348,9 +345,13 @@ __global__ void __launch_bounds__(CB *G, MINB) batch_field_kernel(BatchArgs a) {
                     bool near;
                     plan.chunk(c, start, len, near);
                     const float4 *hb = st.hib + ((seq + c) % kStages) * kCH;
-                    if (pass == 2) far_chunk_fwd_outer<P, 16>(hb, stf, len, g, ux, uy, uz, acc);
-                    else if (pass) far_chunk_fwd<P, 16, true>(hb, stf, len, g, ux, uy, uz, acc, shift_sum);
-                    else far_chunk_fwd<P, 16, false>(hb, stf, len, g, ux, uy, uz, acc, shift_sum);
+                    if (pass && sym)
+                        far_chunk_fwd<P, 16, true, true>(hb, stf, len, g, ux, uy, uz, acc,
+                                                         shift_sum, outer_at - start);
+                    else if (pass)
+                        far_chunk_fwd<P, 16, true>(hb, stf, len, g, ux, uy, uz, acc, shift_sum);
+                    else
+                        far_chunk_fwd<P, 16, false>(hb, stf, len, g, ux, uy, uz, acc, shift_sum);
                     stage_next(st, plan, y.hi, y.lo, c, seq);
                 }
                 seq += plan.n_chunks;

@@ -495,13 +495,21 @@ __device__ __forceinline__ void far_chunk(const float4 *hb, const float4 *stf, i
 // partials over FLUSH entries are flushed into the FP64 acc.  Shell entries
 // beyond every site's cutoff (the list radius carries the region radius on
 // top) are skipped: they would add exactly nothing.
-template <int P, int FLUSH, bool MASK>
+// OUTER (symmetric sites, MASK): entries [outer_from, len) are outer shell
+// entries (RegionInfo::n_outer: |d0| > rc for every pose center of the
+// region), where a director's site on the far side of the center has q >=
+// |d0|^2 + o^2 > rc^2 and adds exact zeros; only the near site (q = |d0|^2 +
+// o^2 - |2 o t|, the same FP32 fma as its two-site q) is evaluated there, so
+// the partials, and the result, are bit for bit those of the two-site loop.
+template <int P, int FLUSH, bool MASK, bool OUTER = false>
 __device__ __forceinline__ void far_chunk_fwd(const float4 *hb, const float4 *stf, int len,
                                               const FarGeom &g, const float2 (&ux)[P / 2],
                                               const float2 (&uy)[P / 2],
                                               const float2 (&uz)[P / 2], double (&acc)[P],
-                                              double &shift_sum) {
+                                              double &shift_sum, int outer_from = 0) {
+    static_assert(!OUTER || MASK, "outer entries are shell entries");
     constexpr int PP = P / 2;
+    const float2 nam = make_float2(-fabsf(g.m0.x), -fabsf(g.m0.x));   // -|m0|
 #pragma unroll 1
     for (int e0 = 0; e0 < len; e0 += FLUSH) {
         float2 fa[PP];
@@ -509,8 +517,9 @@ __device__ __forceinline__ void far_chunk_fwd(const float4 *hb, const float4 *st
 #pragma unroll
         for (int j = 0; j < PP; ++j) fa[j] = make_float2(0.f, 0.f);
         const int e1 = min(e0 + FLUSH, len);
+        const int em = OUTER ? max(e0, min(e1, outer_from)) : e1;
 #pragma unroll 2
-        for (int e = e0; e < e1; ++e) {
+        for (int e = e0; e < em; ++e) {
             float2 k0, k1, dx2, dy2, dz2, c12, mc6, sh;
             {
                 const float4 h = hb[e];
@@ -549,68 +558,42 @@ __device__ __forceinline__ void far_chunk_fwd(const float4 *hb, const float4 *st
                 }
             }
         }
+        if (OUTER) {
+#pragma unroll 2
+            for (int e = em; e < e1; ++e) {   // outer entries: the near site alone
+                float2 k0, dx2, dy2, dz2, c12, mc6, sh;
+                {
+                    const float4 h = hb[e];
+                    const float4 tp = stf[__float_as_int(h.w)];
+                    const float dx = h.x - g.cx, dy = h.y - g.cy, dz = h.z - g.cz;
+                    const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    if (dd > g.out2) continue;
+                    k0 = make_float2(dd + g.oo0, dd + g.oo0);
+                    dx2 = make_float2(dx, dx);
+                    dy2 = make_float2(dy, dy);
+                    dz2 = make_float2(dz, dz);
+                    c12 = make_float2(tp.x, tp.x);
+                    mc6 = make_float2(-tp.y, -tp.y);
+                    sh = make_float2(tp.z, tp.z);
+                }
+#pragma unroll
+                for (int j = 0; j < PP; ++j) {
+                    const float2 t =
+                        __ffma2_rn(dx2, ux[j], __ffma2_rn(dy2, uy[j], __fmul2_rn(dz2, uz[j])));
+                    const float2 d2 = __ffma2_rn(nam, make_float2(fabsf(t.x), fabsf(t.y)), k0);
+                    float r0, r1;
+                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(d2.x));
+                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r1) : "f"(d2.y));
+                    const float2 n1 = make_float2(r0, r1);
+                    float2 n3 = __fmul2_rn(__fmul2_rn(n1, n1), n1);
+                    const float2 m = make_float2(set_lt(d2.x, g.rc2f), set_lt(d2.y, g.rc2f));
+                    n3 = __fmul2_rn(n3, m);
+                    fa[j] = __ffma2_rn(m, sh, fa[j]);
+                    fa[j] = __ffma2_rn(n3, __ffma2_rn(c12, n3, mc6), fa[j]);
+                }
+            }
+        }
         if (!MASK) shift_sum += (double)fs;
-#pragma unroll
-        for (int j = 0; j < PP; ++j) {
-            acc[2 * j] += (double)fa[j].x;
-            acc[2 * j + 1] += (double)fa[j].y;
-        }
-    }
-}
-
-// Forward far chunk over outer shell entries (RegionInfo::n_outer: |d0| >
-// rc for every pose center of the region), symmetric sites (o_1 = -o_0):
-// only a director's site on the entry's side can be inside the cutoff, q =
-// |d0|^2 + o^2 - |2 o t|, so only that one is evaluated (masked as in
-// far_chunk_fwd); the other adds exactly nothing there too.  (The batched
-// forward kernel takes it; in the per-field far kernel, bounded to 80
-// registers, the third pass cost spills and more time than it saved.)
-template <int P, int FLUSH, int UNROLL = 2>
-__device__ __forceinline__ void far_chunk_fwd_outer(const float4 *hb, const float4 *stf, int len,
-                                                    const FarGeom &g, const float2 (&ux)[P / 2],
-                                                    const float2 (&uy)[P / 2],
-                                                    const float2 (&uz)[P / 2],
-                                                    double (&acc)[P]) {
-    constexpr int PP = P / 2;
-    const float2 nam = make_float2(-fabsf(g.m0.x), -fabsf(g.m0.x));   // -|m0|
-#pragma unroll 1
-    for (int e0 = 0; e0 < len; e0 += FLUSH) {
-        float2 fa[PP];
-#pragma unroll
-        for (int j = 0; j < PP; ++j) fa[j] = make_float2(0.f, 0.f);
-        const int e1 = min(e0 + FLUSH, len);
-#pragma unroll UNROLL
-        for (int e = e0; e < e1; ++e) {
-            float2 k0, dx2, dy2, dz2, c12, mc6, sh;
-            {
-                const float4 h = hb[e];
-                const float4 tp = stf[__float_as_int(h.w)];   // (c12, c6, shift, -)
-                const float dx = h.x - g.cx, dy = h.y - g.cy, dz = h.z - g.cz;
-                const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                if (dd > g.out2) continue;
-                k0 = make_float2(dd + g.oo0, dd + g.oo0);
-                dx2 = make_float2(dx, dx);
-                dy2 = make_float2(dy, dy);
-                dz2 = make_float2(dz, dz);
-                c12 = make_float2(tp.x, tp.x);
-                mc6 = make_float2(-tp.y, -tp.y);
-                sh = make_float2(tp.z, tp.z);
-            }
-#pragma unroll
-            for (int j = 0; j < PP; ++j) {
-                const float2 t =
-                    __ffma2_rn(dx2, ux[j], __ffma2_rn(dy2, uy[j], __fmul2_rn(dz2, uz[j])));
-                const float2 d2 = __ffma2_rn(nam, make_float2(fabsf(t.x), fabsf(t.y)), k0);
-                float r0, r1;
-                asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(d2.x));
-                asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r1) : "f"(d2.y));
-                const float2 n1 = make_float2(r0, r1);
-                const float2 m = make_float2(set_lt(d2.x, g.rc2f), set_lt(d2.y, g.rc2f));
-                const float2 n3 = __fmul2_rn(__fmul2_rn(__fmul2_rn(n1, n1), n1), m);
-                fa[j] = __ffma2_rn(m, sh, fa[j]);
-                fa[j] = __ffma2_rn(n3, __ffma2_rn(c12, n3, mc6), fa[j]);
-            }
-        }
 #pragma unroll
         for (int j = 0; j < PP; ++j) {
             acc[2 * j] += (double)fa[j].x;
