@@ -392,8 +392,23 @@ __device__ __forceinline__ void shell_border_repair(const float4 *hi, const floa
     e = 0.0;
 #pragma unroll
     for (int k = 0; k < 6; ++k) g[k] = 0.0;
-    for (int k = first; k < n; k += step) {
-        const float4 h = hi[off + k];
+    // four entries per lane and round, their loads issued together (the
+    // per-entry work is short: one load at a time left the loop waiting on
+    // memory); each lane still visits its entries in increasing order
+    constexpr int kRound = 4;
+#pragma unroll 1
+    for (int k0 = first; k0 < n; k0 += kRound * step) {
+        float4 hv[kRound];
+#pragma unroll
+        for (int i = 0; i < kRound; ++i) {
+            const int k = k0 + i * step;
+            hv[i] = k < n ? hi[off + k] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int i = 0; i < kRound; ++i) {
+        const int k = k0 + i * step;
+        if (k >= n) continue;
+        const float4 h = hv[i];
         const float dx = h.x - f.cx, dy = h.y - f.cy, dz = h.z - f.cz;
         const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
         if (dd > f.out2) continue;
@@ -426,6 +441,7 @@ __device__ __forceinline__ void shell_border_repair(const float4 *hi, const floa
             g[3] += os * de * px;
             g[4] += os * de * py;
             g[5] += os * de * pz;
+        }
         }
     }
 }
