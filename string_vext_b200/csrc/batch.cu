@@ -81,8 +81,9 @@ struct BatchArgs {
 
 // Forward + adjoint item: the same staged pipeline with the AdjAcc pair loops
 // (pair.cuh); writes the energy and [dE/dc, tangent dE/du] of every pose.
-// Far entries come in two passes: inner (no cutoff mask, shift summed once
-// per entry) and shell.
+// Far entries come in two passes, inner (no cutoff mask, shift summed once
+// per entry) and shell, and with OUTER (symmetric sites) a third over the
+// outer shell entries, one site per director (far_chunk_outer).
 // GSUM: the FP64 gradient sums wait in shared memory (gsum) during the far
 // passes, so those passes hold only the energy sums and FP32 partials.
 // BORDER 1: border[p] receives the smallest |q - rc^2| (FP32) of director p
