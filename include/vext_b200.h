@@ -184,6 +184,9 @@ typedef struct {
     int64_t near_entries;
     int64_t refined_poses;
     double list_build_ms, kernel_ms, epilogue_ms;  /* device time (events)   */
+    int64_t outer_entries;   /* shell entries beyond rc + the region radius of
+                                their region's origin (at most one site of a
+                                director inside the cutoff)                   */
 } vext_field_stats;
 
 /* Full Vext field on a size^3 fractional grid (centers ((i+.5)/S, ...),

@@ -49,7 +49,8 @@ class FieldStats(ctypes.Structure):
     _fields_ = [("poses", ctypes.c_int64), ("regions", ctypes.c_int64),
                 ("list_entries", ctypes.c_int64), ("near_entries", ctypes.c_int64),
                 ("refined_poses", ctypes.c_int64), ("list_build_ms", ctypes.c_double),
-                ("kernel_ms", ctypes.c_double), ("epilogue_ms", ctypes.c_double)]
+                ("kernel_ms", ctypes.c_double), ("epilogue_ms", ctypes.c_double),
+                ("outer_entries", ctypes.c_int64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -726,6 +726,7 @@ static int field_device(System *sys, int size, int n_axes, const double *axes_ho
         stats->regions = rs->n_regions;
         stats->list_entries = rs->n_entries;
         stats->near_entries = rs->n_near;
+        stats->outer_entries = rs->n_outer;
         stats->refined_poses = o.mode == VEXT_MODE_MIXED && o.band_hi > o.band_lo ? refined : 0;
         stats->list_build_ms = rs->build_ms;
         stats->kernel_ms = k_ms;

@@ -52,7 +52,7 @@ struct RegionSet {
     // data
     int n_regions = 0;
     int n_ri = 0, n_rj = 0, n_rk = 0;       // regions per axis
-    long long n_entries = 0, n_near = 0;
+    long long n_entries = 0, n_near = 0, n_outer = 0;
     RegionInfo *d_info = nullptr;
     float4 *d_hi = nullptr, *d_lo = nullptr;
     std::vector<RegionInfo> h_info;

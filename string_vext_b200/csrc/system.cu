@@ -299,14 +299,16 @@ static int build_lists(System *sys, RegionSet *rs, cudaStream_t stream) {
     VEXT_CUDA(cudaMemcpyAsync(rs->h_info.data(), rs->d_info, sizeof(RegionInfo) * n,
                               cudaMemcpyDeviceToHost, stream));
     VEXT_CUDA(cudaStreamSynchronize(stream));
-    long long off = 0, near = 0;
+    long long off = 0, near = 0, outer = 0;
     for (auto &r : rs->h_info) {
         r.off = off;
         off += r.n_total;
         near += r.n_near;
+        outer += r.n_outer;
     }
     rs->n_entries = off;
     rs->n_near = near;
+    rs->n_outer = outer;
     VEXT_CUDA(cudaMemcpyAsync(rs->d_info, rs->h_info.data(), sizeof(RegionInfo) * n,
                               cudaMemcpyHostToDevice, stream));
     if (off > rs->capacity || !rs->d_hi) {

@@ -192,3 +192,25 @@ def test_off_center_sites_forward_field():
             mixed = system.field(4, axes, mode=MIXED, energy=True)["energy"]
         assert rel(e64, ref).max() < 1e-10
         assert_mixed_ok(mixed, ref)
+
+
+def test_list_classes_cover_the_outer_shell():
+    """Every region's shell ends with its outer entries (beyond rc + the region
+    radius of the origin, where at most one site of a director is inside the
+    cutoff and the batched kernels evaluate that site alone).  On full_field
+    they are a sizeable part of the list, they lie beyond the near class, and
+    the per-field path (which evaluates both sites there) still matches the
+    FP64 oracle on a sample of poses whose pairs reach into them."""
+    case = synth.full_field()
+    size = 6
+    centers, axes = regular_pose_grid(size, 64)
+    axes = normalized_directors(axes)
+    with VextSystem(case) as system:
+        out = system.field(size, axes, energy=True, orientation=False)
+        st = system.last_stats
+    assert 0 < st["outer_entries"] < st["list_entries"] - st["near_entries"]
+    # the outer shell of a 16-center region: rc + rho + 1e-3 A to rc + max|o| + rho,
+    # about a tenth of the list
+    assert 0.05 < st["outer_entries"] / st["list_entries"] < 0.3
+    pick = np.arange(0, len(centers), 37)
+    assert_mixed_ok(out["energy"][pick], oracle.pose_energy(case, centers[pick], axes))
