@@ -182,8 +182,10 @@ __device__ __forceinline__ void block_scan2(int a, int b, int &pa, int &pb, int 
 
 constexpr int kBuildThreads = 256;
 
+// Per region: the entries of each class, and per thread (atoms j = tid, tid +
+// kBuildThreads, ...) its (near, inner, shell, outer) counts for the fill.
 __global__ void __launch_bounds__(kBuildThreads)
-    region_count_kernel(BuildArgs a, RegionInfo *regs, int n_regions) {
+    region_count_kernel(BuildArgs a, RegionInfo *regs, int n_regions, int4 *counts) {
     const int region = blockIdx.x;
     if (region >= n_regions) return;
     const RegionInfo r = regs[region];
@@ -198,6 +200,8 @@ __global__ void __launch_bounds__(kBuildThreads)
             inner += q >= rn2 && q < ri2;
             outer += q >= rn2 && q >= ri2 && q >= ro2;
         });
+    counts[(long long)region * kBuildThreads + threadIdx.x] =
+        make_int4(near, inner, total - near - inner - outer, outer);
     __shared__ int sh[128];
     int pa, pb, ta, tb, pc, pd, tc, td;
     block_scan2<kBuildThreads>(near, total, pa, pb, ta, tb, sh);
@@ -210,9 +214,13 @@ __global__ void __launch_bounds__(kBuildThreads)
     }
 }
 
-__global__ void __launch_bounds__(kBuildThreads)
-    region_fill_kernel(BuildArgs a, const RegionInfo *regs, int n_regions, float4 *hi, float4 *lo,
-                       int *status) {
+// Entry order inside each class: thread-major (thread t's atoms t, t +
+// kBuildThreads, ... in turn, each atom's images in enumeration order), so a
+// thread's slots follow from a block scan of the per-thread counts that
+// region_count_kernel stored and the candidates are enumerated once here.
+__global__ void __launch_bounds__(kBuildThreads, 2)
+    region_fill_kernel(BuildArgs a, const RegionInfo *regs, int n_regions, const int4 *counts,
+                       float4 *hi, float4 *lo, int *status) {
     const int region = blockIdx.x;
     if (region >= n_regions) return;
     const RegionInfo r = regs[region];
@@ -220,51 +228,35 @@ __global__ void __launch_bounds__(kBuildThreads)
     const double ri = a.r_inner0 - r.rho, ri2 = ri > 0 ? ri * ri : 0.0;
     const double ro = a.r_outer0 + r.rho, ro2 = ro * ro;
     __shared__ int sh[128];
-    // entry order: near | far inner | far shell | outer shell, atom-major
-    // inside each class
+    // entry order: near | far inner | far shell | outer shell
     const int end_shell = r.n_total - r.n_outer;
-    int base_near = 0, base_inner = r.n_near, base_shell = r.n_near + r.n_inner,
-        base_outer = end_shell;
-    for (int j0 = 0; j0 < a.n_atoms; j0 += kBuildThreads) {
-        const int j = j0 + threadIdx.x;
-        int near = 0, inner = 0, shell = 0, outer = 0;
-        if (j < a.n_atoms)
-            for_each_image(a, r, j, rl, [&](double q, double, double, double) {
-                if (q < rn2) ++near;
-                else if (q < ri2) ++inner;
-                else if (q < ro2) ++shell;
-                else ++outer;
-            });
-        int pn, pi, tn, ti, ps, po, ts, to;
-        block_scan2<kBuildThreads>(near, inner, pn, pi, tn, ti, sh);
-        block_scan2<kBuildThreads>(shell, outer, ps, po, ts, to, sh);
-        if (j < a.n_atoms) {
-            int wn = base_near + pn, wi = base_inner + pi, ws = base_shell + ps,
-                wo = base_outer + po;
-            const int t = a.type[j];
-            for_each_image(a, r, j, rl, [&](double q, double x, double y, double z) {
-                const int cls = q < rn2 ? 0 : (q < ri2 ? 1 : (q < ro2 ? 2 : 3));
-                const int slot = cls == 0 ? wn++ : (cls == 1 ? wi++ : (cls == 2 ? ws++ : wo++));
-                const int end = cls == 0 ? r.n_near
-                                         : (cls == 1 ? r.n_near + r.n_inner
-                                                     : (cls == 2 ? end_shell : r.n_total));
-                if (slot >= end) {
-                    atomicExch(status, DEV_BAD_LIST);
-                    return;
-                }
-                const float hx = (float)x, hy = (float)y, hz = (float)z;
-                hi[r.off + slot] = make_float4(hx, hy, hz, __int_as_float(t));
-                lo[r.off + slot] = make_float4((float)(x - hx), (float)(y - hy), (float)(z - hz), 0.f);
-            });
-        }
-        base_near += tn;
-        base_inner += ti;
-        base_shell += ts;
-        base_outer += to;
-    }
-    if (threadIdx.x == 0 && (base_near != r.n_near || base_inner != r.n_near + r.n_inner ||
-                             base_shell != end_shell || base_outer != r.n_total))
+    const int4 c = counts[(long long)region * kBuildThreads + threadIdx.x];
+    int pn, pi, tn, ti, ps, po, ts, to;
+    block_scan2<kBuildThreads>(c.x, c.y, pn, pi, tn, ti, sh);
+    block_scan2<kBuildThreads>(c.z, c.w, ps, po, ts, to, sh);
+    if (threadIdx.x == 0 && (tn != r.n_near || ti != r.n_inner ||
+                             ts != end_shell - r.n_near - r.n_inner || to != r.n_outer))
         atomicExch(status, DEV_BAD_LIST);
+    // this thread's next slot and end per class (scalars: an indexed array
+    // would live in local memory)
+    int wn = pn, wi = r.n_near + pi, ws = r.n_near + r.n_inner + ps, wo = end_shell + po;
+    const int en = wn + c.x, ei = wi + c.y, es = ws + c.z, eo = wo + c.w;
+    for (int j = threadIdx.x; j < a.n_atoms; j += kBuildThreads) {
+        const int t = a.type[j];
+        for_each_image(a, r, j, rl, [&](double q, double x, double y, double z) {
+            const int cls = q < rn2 ? 0 : (q < ri2 ? 1 : (q < ro2 ? 2 : 3));
+            const int slot = cls == 0 ? wn++ : (cls == 1 ? wi++ : (cls == 2 ? ws++ : wo++));
+            const int lim = cls == 0 ? en : (cls == 1 ? ei : (cls == 2 ? es : eo));
+            if (slot >= lim) {
+                atomicExch(status, DEV_BAD_LIST);
+                return;
+            }
+            const float hx = (float)x, hy = (float)y, hz = (float)z;
+            hi[r.off + slot] = make_float4(hx, hy, hz, __int_as_float(t));
+            lo[r.off + slot] = make_float4((float)(x - hx), (float)(y - hy), (float)(z - hz), 0.f);
+        });
+    }
+    if (wn != en || wi != ei || ws != es || wo != eo) atomicExch(status, DEV_BAD_LIST);
 }
 
 // ------------------------------------------------------------ region sets
@@ -275,7 +267,31 @@ RegionSet::~RegionSet() {
     cudaFree(d_lo);
 }
 
+// Per-device scratch of the per-(region, thread) class counts that the count
+// pass hands to the fill pass; one list build at a time uses it (the lock is
+// held until the build's kernels have finished).
+namespace {
+struct BuildScratch {
+    std::mutex lock;
+    int4 *ptr = nullptr;
+    size_t cap = 0;
+};
+BuildScratch &build_scratch(int device) {
+    static BuildScratch scratch[64];
+    return scratch[device & 63];
+}
+// Waits for the stream before the scratch lock is released, also on the
+// early error returns of build_lists.
+struct StreamDrain {
+    cudaStream_t stream;
+    ~StreamDrain() { cudaStreamSynchronize(stream); }
+};
+}  // namespace
+
 static int build_lists(System *sys, RegionSet *rs, cudaStream_t stream) {
+    BuildScratch &scratch = build_scratch(sys->device);
+    std::lock_guard<std::mutex> scratch_guard(scratch.lock);
+    StreamDrain drain{stream};
     BuildArgs a;
     a.H = sys->H;
     for (int k = 0; k < 3; ++k) a.einv[k] = sys->einv[k];
@@ -294,7 +310,8 @@ static int build_lists(System *sys, RegionSet *rs, cudaStream_t stream) {
                               cudaMemcpyHostToDevice, stream));
     cudaEvent_t e0 = sys->ev[3], e1 = sys->ev[4];
     VEXT_CUDA(cudaEventRecord(e0, stream));
-    region_count_kernel<<<n, kBuildThreads, 0, stream>>>(a, rs->d_info, n);
+    VEXT_TRY(ensure_capacity(scratch.ptr, scratch.cap, (size_t)n * kBuildThreads));
+    region_count_kernel<<<n, kBuildThreads, 0, stream>>>(a, rs->d_info, n, scratch.ptr);
     VEXT_CUDA(cudaGetLastError());
     VEXT_CUDA(cudaMemcpyAsync(rs->h_info.data(), rs->d_info, sizeof(RegionInfo) * n,
                               cudaMemcpyDeviceToHost, stream));
@@ -320,8 +337,8 @@ static int build_lists(System *sys, RegionSet *rs, cudaStream_t stream) {
         VEXT_CUDA(cudaMalloc(&rs->d_lo, sizeof(float4) * std::max<long long>(off, 1)));
         rs->capacity = std::max<long long>(off, 1);
     }
-    region_fill_kernel<<<n, kBuildThreads, 0, stream>>>(a, rs->d_info, n, rs->d_hi, rs->d_lo,
-                                                        sys->d_status);
+    region_fill_kernel<<<n, kBuildThreads, 0, stream>>>(a, rs->d_info, n, scratch.ptr, rs->d_hi,
+                                                        rs->d_lo, sys->d_status);
     VEXT_CUDA(cudaGetLastError());
     VEXT_CUDA(cudaEventRecord(e1, stream));
     VEXT_CUDA(cudaEventSynchronize(e1));
