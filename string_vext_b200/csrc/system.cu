@@ -12,6 +12,8 @@
 // fractional extent of a ball of radius R is R |Hinv[:,k]|, so n_k runs over
 // [ceil(-d_k - R e_k), floor(-d_k + R e_k)] with d = f_j - f_o; the exact
 // distance test is done in FP64 on (d + n) @ H.  No minimum image is used.
+#include <cuda.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -269,13 +271,42 @@ RegionSet::~RegionSet() {
 
 // Per-device scratch of the per-(region, thread) class counts that the count
 // pass hands to the fill pass; one list build at a time uses it (the lock is
-// held until the build's kernels have finished).
+// held until the build's kernels have finished).  It belongs to the context
+// it was allocated in: after a device reset (a new context, told apart by
+// its unique id) the old array is gone and a new one is allocated.
 namespace {
 struct BuildScratch {
     std::mutex lock;
     int4 *ptr = nullptr;
     size_t cap = 0;
+    unsigned long long ctx_id = 0;
 };
+// Unique id of the calling thread's current context (0 when unavailable).
+unsigned long long current_context_id() {
+    using GetCurrentFn = CUresult (*)(CUcontext *);
+    using GetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+    static const std::pair<GetCurrentFn, GetIdFn> fns = [] {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa = cudaDriverEntryPointSymbolNotFound, qb = qa;
+        const bool ok =
+            cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) ==
+                cudaSuccess &&
+            qa == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) == cudaSuccess &&
+            qb == cudaDriverEntryPointSuccess;
+        if (!ok) {
+            cudaGetLastError();
+            return std::pair<GetCurrentFn, GetIdFn>(nullptr, nullptr);
+        }
+        return std::pair<GetCurrentFn, GetIdFn>(reinterpret_cast<GetCurrentFn>(a),
+                                                reinterpret_cast<GetIdFn>(b));
+    }();
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!fns.first || fns.first(&ctx) != CUDA_SUCCESS || !ctx || fns.second(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
 BuildScratch &build_scratch(int device) {
     static BuildScratch scratch[64];
     return scratch[device & 63];
@@ -310,7 +341,15 @@ static int build_lists(System *sys, RegionSet *rs, cudaStream_t stream) {
                               cudaMemcpyHostToDevice, stream));
     cudaEvent_t e0 = sys->ev[3], e1 = sys->ev[4];
     VEXT_CUDA(cudaEventRecord(e0, stream));
+    const unsigned long long ctx = current_context_id();
+    if (scratch.ptr && ctx != 0 && scratch.ctx_id != 0 && ctx != scratch.ctx_id) {
+        // allocated in a context that has since been reset: it went with that
+        // context; allocate anew
+        scratch.ptr = nullptr;
+        scratch.cap = 0;
+    }
     VEXT_TRY(ensure_capacity(scratch.ptr, scratch.cap, (size_t)n * kBuildThreads));
+    scratch.ctx_id = ctx;
     region_count_kernel<<<n, kBuildThreads, 0, stream>>>(a, rs->d_info, n, scratch.ptr);
     VEXT_CUDA(cudaGetLastError());
     VEXT_CUDA(cudaMemcpyAsync(rs->h_info.data(), rs->d_info, sizeof(RegionInfo) * n,
