@@ -13,7 +13,7 @@
 namespace vext {
 
 constexpr int kCH = 128;      // entries per chunk
-constexpr int kStages = 3;    // pipeline depth
+constexpr int kStages = 4;    // pipeline depth (3: 1 % slower forward + adjoint)
 
 struct ChunkPlan {
     long long off;
